@@ -1,0 +1,123 @@
+/*
+ * vfb.h -- C ABI of the B200-native VFB engine (libvfb_b200.so).
+ *
+ * Learns the smallest LTL formula over  AP | ~f | f&g | f|g | Xf | Ff | Gf | fUg
+ * that holds at step 0 of every positive trace and fails at step 0 of every
+ * negative trace, by bottom-up enumeration with a per-level characteristic-set
+ * cache and semantic deduplication on one GPU.
+ *
+ * Plain C types only; no exceptions or C++ types cross this boundary.  Every
+ * entry point returns a vfb_status.  A context is not thread-safe: use one per
+ * host thread (or serialise calls).
+ *
+ * Reference interfaces these entry points replace (SynthesisLab/VFB):
+ *   vfb_solve        std::string LTL(maxLen, inputData, traceLen, traceLength)
+ *                    ltl_nocache.cu:319-446, with the search of
+ *                    std::string LTLI(...) LTL_BS.cu:1069-1532 (cached,
+ *                    deduplicated enumeration); same input layout
+ *                    inputData[trace*numVar + var] (ltl_nocache.cu:51-65)
+ *   vfb_read_json    readJsonFile  ltl_nocache.cu:35-76
+ *   vfb_format_infix LTLToString   ltl_nocache.cu:289-317
+ *   vfb_batch_solve  no counterpart (the reference solves one instance per
+ *                    process); results equal one vfb_solve per instance
+ *   vfb_create / vfb_destroy  replace the reference's process-global state
+ *                    (__constant__ symbols, cudaMalloc'd caches) with a context
+ */
+#ifndef VFB_H
+#define VFB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VFB_MAX_SIZE 32      /* formula size limit (ltl_nocache.cu:11) */
+#define VFB_MAX_TRACES 128
+#define VFB_MAX_VARS 64
+#define VFB_MAX_LENGTH 64    /* one uint64 word per trace (ltl_nocache.cu:12) */
+
+typedef enum {
+  VFB_OK = 0,            /* formula found */
+  VFB_NOT_FOUND = 1,     /* no formula up to max_size ("Not found !", ltl_nocache.cu:439) */
+  VFB_LIMIT = 2,         /* input outside the supported limits */
+  VFB_OOM = 3,           /* device memory budget exhausted */
+  VFB_DEVICE_ERROR = 4,  /* CUDA error, missing device or kernel image */
+  VFB_TIMEOUT = 5,       /* reserved for the serving loop */
+  VFB_BAD_INPUT = 6      /* malformed arguments or JSON */
+} vfb_status;
+
+/* Operator tokens in results: token >= 0 is a proposition index; token < 0 is
+ * -(1 + i) for operator i of "~&|XFGU" (the reference's Op order, LTL_BS.cu:17). */
+#define VFB_TOK_OP(i) (-(1 + (i)))
+
+typedef struct {
+  int device;              /* CUDA device ordinal */
+  size_t mem_limit_bytes;  /* device memory budget of one solve/batch (0: 90% of free memory) */
+  int verbose;             /* 1: per-level progress lines on stderr */
+} vfb_opts;
+
+/* One learning problem.  Layout as ltl_nocache's readJsonFile: words[i*num_vars + v]
+ * holds proposition v on trace i (bit t = value at step t); traces 0..num_pos-1
+ * are positive, the rest negative; lengths[i] is trace i's length (1..64). */
+typedef struct {
+  int num_vars;
+  int num_traces;
+  int num_pos;
+  const uint64_t *words;
+  const int *lengths;
+  int max_size;            /* 1..32 */
+  int rlx_type;            /* relaxed-uniqueness rule when total trace bits exceed 126:
+                              1 strided sample, 2 proportional prefix, 3 hash (default,
+                              0 means 3); LTL_BS.cu:30-110 */
+} vfb_instance;
+
+typedef struct {
+  vfb_status status;
+  int size;                          /* formula size, or last level searched */
+  int rpn_len;
+  int16_t rpn[VFB_MAX_SIZE];         /* RPN tokens, see VFB_TOK_OP */
+  uint64_t level_rows[VFB_MAX_SIZE + 1];   /* unique characteristic sets per size (index = size);
+                                              the final size counts up to the solution */
+  uint64_t level_cands[VFB_MAX_SIZE + 1];  /* candidates evaluated per size */
+  uint64_t total_rows;               /* sum of level_rows */
+  uint64_t solution_index;           /* canonical index of the solution within its size */
+  double seconds;                    /* wall time of the call (batch: of the whole batch) */
+} vfb_result;
+
+vfb_status vfb_create(void **ctx, const vfb_opts *opts);
+void vfb_destroy(void *ctx);
+
+vfb_status vfb_solve(void *ctx, const vfb_instance *inst, vfb_result *out);
+
+/* Solves n independent instances together; out[i] equals vfb_solve(inst[i]). */
+vfb_status vfb_batch_solve(void *ctx, const vfb_instance *inst, int n, vfb_result *out);
+
+/* Human-readable name of a status. */
+const char *vfb_status_str(vfb_status s);
+
+/* ----------------------------------------------------------- trace JSON input
+ * Parses a trace file in the reference's JSON schema (keys
+ * number_atomic_propositions, number_traces, number_positive_traces,
+ * max_length_traces, atomic_propositions, positive_traces, negative_traces).
+ * On success *out is a library-owned problem; free it with vfb_json_free. */
+typedef struct {
+  vfb_instance inst;
+  int max_length_traces;   /* the file's declared maximum length */
+  char **names;            /* num_vars proposition names */
+} vfb_json_problem;
+
+vfb_status vfb_read_json(const char *path, vfb_json_problem **out, char *err, size_t errlen);
+void vfb_json_free(vfb_json_problem *p);
+
+/* Infix text of a result's formula in the reference's notation: "~(x)",
+ * "X(x)", "(l) & (r)", "(l) U (r)" (ltl_nocache.cu:289-317).  Writes at most
+ * buflen bytes including the terminator; returns the full length needed, or
+ * -1 if the RPN is malformed. */
+int vfb_format_infix(const vfb_result *r, const char *const *names, char *buf, size_t buflen);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,59 @@
+"""Seeded test instances shared by the CPU and GPU tests."""
+from __future__ import annotations
+
+from vfb_b200 import synth
+
+
+def random_instance(seed: int, num_vars: int, n_pos: int, n_neg: int, lengths, max_size: int,
+                    p: float = 0.5, rlx_type: int = 3) -> synth.Instance:
+    """Unlabelled random traces (no planted formula); lengths: int or list per trace."""
+    rng = synth.Rng(seed)
+    n = n_pos + n_neg
+    lens = lengths if isinstance(lengths, list) else [lengths] * n
+    traces = []
+    for i in range(n):
+        traces.append((lens[i], [rng.bernoulli_word(lens[i], p) for _ in range(num_vars)]))
+    return synth.Instance(num_vars, traces[:n_pos], traces[n_pos:], max_size,
+                          [f"p{v}" for v in range(num_vars)], None, rlx_type, f"rand{seed}")
+
+
+def small_exact_cases():
+    """Instances with at most 126 trace bits (exact keys), minimal size <= ~7."""
+    out = [synth.config_small()]
+    for s in range(12):
+        rng = synth.Rng(1000 + s)
+        a = 1 + rng.below(3)
+        npos = 1 + rng.below(3)
+        nneg = 1 + rng.below(3)
+        lens = [1 + rng.below(6) for _ in range(npos + nneg)]
+        out.append(random_instance(2000 + s, a, npos, nneg, lens, 7))
+    return out
+
+
+def relaxed_cases(rlx_type: int):
+    """Instances with more than 126 trace bits (relaxed keys)."""
+    out = []
+    for s in range(4):
+        rng = synth.Rng(3000 + s)
+        a = 2 + rng.below(2)
+        npos = 4 + rng.below(4)
+        nneg = 4 + rng.below(4)
+        lens = [8 + rng.below(17) for _ in range(npos + nneg)]
+        out.append(random_instance(4000 + s, a, npos, nneg, lens, 6, rlx_type=rlx_type))
+    return out
+
+
+def planted_cases(count: int = 6, max_size_extra: int = 2):
+    """Planted-formula instances (labels from a uniformly drawn formula)."""
+    out = []
+    for s in range(count):
+        rng = synth.Rng(5000 + s)
+        a = 2 + rng.below(3)
+        size = 4 + rng.below(4)
+        t = 6 + rng.below(20)
+        npos = t // 2
+        inst = synth.planted_instance(rng, a, size, npos, t - npos,
+                                      lambda: 4 + rng.below(29), 0.5, size + max_size_extra,
+                                      name=f"planted{s}")
+        out.append(inst)
+    return out

@@ -1,0 +1,104 @@
+"""GPU parity: the CUDA engine (through the C ABI) against the CPU oracle.
+
+Bit-exact: same status, minimal size, returned formula (RPN), per-size unique
+counts, candidates evaluated and canonical solution index.
+"""
+import os
+import subprocess
+
+import pytest
+
+import oracle
+import vfb_b200
+from vfb_b200 import synth
+from tests import cases
+
+pytestmark = pytest.mark.gpu
+
+
+def _check(engine, inst, **kw):
+    prob = vfb_b200.Problem.from_instance(inst)
+    for k, v in kw.items():
+        setattr(prob, k, v)
+    got = engine.solve(prob)
+    ref = oracle.solve(oracle.Problem.from_instance(inst, rlx_type=prob.rlx_type,
+                                                    max_size=prob.max_size))
+    status = {oracle.FOUND: vfb_b200.OK, oracle.NOT_FOUND: vfb_b200.NOT_FOUND}[ref["status"]]
+    assert got.status == status
+    assert got.size == ref["size"]
+    assert got.rpn == ref["rpn"]
+    assert got.level_rows == ref["level_rows"]
+    assert got.level_cands == ref["level_cands"]
+    if got.status == vfb_b200.OK:
+        assert got.solution_index == ref["solution_index"]
+        ok, _ = oracle.eval_rpn(oracle.Problem.from_instance(inst), got.rpn)
+        assert ok == 1
+    return got
+
+
+def test_small_config(engine):
+    _check(engine, synth.config_small())
+
+
+@pytest.mark.parametrize("inst", cases.small_exact_cases(), ids=lambda i: i.name)
+def test_exact_keys(engine, inst):
+    _check(engine, inst)
+
+
+@pytest.mark.parametrize("rlx", [1, 2, 3])
+def test_relaxed_keys(engine, rlx):
+    for inst in cases.relaxed_cases(rlx):
+        _check(engine, inst, rlx_type=rlx)
+
+
+@pytest.mark.parametrize("inst", cases.planted_cases(), ids=lambda i: i.name)
+def test_planted(engine, inst):
+    got = _check(engine, inst)
+    assert got.size <= len(inst.planted)
+
+
+def test_planted_config(engine):
+    _check(engine, synth.config_planted())
+
+
+def test_not_found_runs_every_level(engine):
+    inst = cases.random_instance(77, 3, 3, 3, 6, 5)
+    inst.neg[0] = inst.pos[0]          # a positive equal to a negative: unsolvable
+    got = _check(engine, inst)
+    assert got.status == vfb_b200.NOT_FOUND and got.size == 5
+
+
+def test_length_64_traces(engine):
+    inst = cases.random_instance(99, 2, 3, 3, 64, 5, p=0.3)
+    _check(engine, inst)
+
+
+def test_batch_equals_single(engine):
+    insts = cases.planted_cases(5) + cases.small_exact_cases()[:5] + cases.relaxed_cases(3)[:2]
+    probs = [vfb_b200.Problem.from_instance(i) for i in insts]
+    batch = engine.batch_solve(probs)
+    for p, b in zip(probs, batch):
+        s = engine.solve(p)
+        assert (b.status, b.size, b.rpn, b.level_rows, b.level_cands) == \
+               (s.status, s.size, s.rpn, s.level_rows, s.level_cands)
+
+
+def test_growth_path_large_level(engine):
+    """An instance whose levels outgrow every initial buffer (rows, table,
+    bitmap, tentative list) several times."""
+    inst = cases.random_instance(4242, 4, 5, 5, 16, 9)
+    inst.neg[0] = inst.pos[0]          # unsolvable: every level up to 9 is built
+    got = _check(engine, inst)
+    assert got.total_rows > 900_000
+
+
+def test_cli_prints_reference_line(tmp_path):
+    inst = synth.config_planted()
+    path = tmp_path / "planted.json"
+    inst.write_json(str(path))
+    out = subprocess.run([vfb_b200.CLI_PATH, str(path), "13"], capture_output=True, text=True,
+                         timeout=120)
+    assert out.returncode == 0
+    ref = oracle.solve(oracle.Problem.from_instance(inst))
+    expect = synth.rpn_to_infix(ref["rpn"], inst.names)
+    assert out.stdout == f"{path}, {expect}\n"

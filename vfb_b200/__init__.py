@@ -1,0 +1,260 @@
+"""vfb_b200 -- B200-native bottom-up LTL formula learning (VFB's cached search).
+
+Python host-side binding of the C ABI in include/vfb.h (libvfb_b200.so).  The
+entry points mirror the reference's host interface:
+
+  ltl(max_len, input_data, trace_len, num_vars, num_pos, names)
+      -> the formula string, "Not found !" or raises; same arguments and
+         meaning as std::string LTL(maxLen, inputData, traceLen, traceLength)
+         of ltl_nocache.cu:319 (whose inputs are globals there).
+  read_json_file(path) -> Problem       (readJsonFile, ltl_nocache.cu:35-76)
+  Engine.solve / Engine.batch_solve     (vfb_solve / vfb_batch_solve)
+
+The search itself runs only in the CUDA library: there is no CPU fallback, and
+importing the engine on a machine without the built library or a B200 raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libvfb_b200.so")
+CLI_PATH = os.path.join(HERE, "_lib", "vfb")
+OPS = "~&|XFGU"
+MAX_SIZE = 32
+
+OK, NOT_FOUND, LIMIT, OOM, DEVICE_ERROR, TIMEOUT, BAD_INPUT = range(7)
+STATUS_NAMES = ["ok", "not found", "limit", "oom", "device error", "timeout", "bad input"]
+
+
+class VfbError(RuntimeError):
+    pass
+
+
+class _Opts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("mem_limit_bytes", ctypes.c_size_t),
+                ("verbose", ctypes.c_int)]
+
+
+class _Instance(ctypes.Structure):
+    _fields_ = [("num_vars", ctypes.c_int), ("num_traces", ctypes.c_int),
+                ("num_pos", ctypes.c_int), ("words", ctypes.POINTER(ctypes.c_uint64)),
+                ("lengths", ctypes.POINTER(ctypes.c_int)), ("max_size", ctypes.c_int),
+                ("rlx_type", ctypes.c_int)]
+
+
+class _Result(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("size", ctypes.c_int), ("rpn_len", ctypes.c_int),
+                ("rpn", ctypes.c_int16 * MAX_SIZE),
+                ("level_rows", ctypes.c_uint64 * (MAX_SIZE + 1)),
+                ("level_cands", ctypes.c_uint64 * (MAX_SIZE + 1)),
+                ("total_rows", ctypes.c_uint64), ("solution_index", ctypes.c_uint64),
+                ("seconds", ctypes.c_double)]
+
+
+class _JsonProblem(ctypes.Structure):
+    _fields_ = [("inst", _Instance), ("max_length_traces", ctypes.c_int),
+                ("names", ctypes.POINTER(ctypes.c_char_p))]
+
+
+EXPORTS = ["vfb_create", "vfb_destroy", "vfb_solve", "vfb_batch_solve", "vfb_status_str",
+           "vfb_read_json", "vfb_json_free", "vfb_format_infix"]
+
+_lib = None
+
+
+def load_library():
+    """Load libvfb_b200.so (building it first if the sources are newer)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        try:
+            from . import build as _build
+            _build.build()
+        except Exception as e:  # noqa: BLE001
+            raise VfbError(f"libvfb_b200.so is missing and could not be built: {e}") from e
+    lib = ctypes.CDLL(LIB_PATH)
+    lib.vfb_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(_Opts)]
+    lib.vfb_create.restype = ctypes.c_int
+    lib.vfb_destroy.argtypes = [ctypes.c_void_p]
+    lib.vfb_destroy.restype = None
+    lib.vfb_solve.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Instance), ctypes.POINTER(_Result)]
+    lib.vfb_solve.restype = ctypes.c_int
+    lib.vfb_batch_solve.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Instance), ctypes.c_int,
+                                    ctypes.POINTER(_Result)]
+    lib.vfb_batch_solve.restype = ctypes.c_int
+    lib.vfb_status_str.argtypes = [ctypes.c_int]
+    lib.vfb_status_str.restype = ctypes.c_char_p
+    lib.vfb_read_json.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.POINTER(_JsonProblem)),
+                                  ctypes.c_char_p, ctypes.c_size_t]
+    lib.vfb_read_json.restype = ctypes.c_int
+    lib.vfb_json_free.argtypes = [ctypes.POINTER(_JsonProblem)]
+    lib.vfb_json_free.restype = None
+    lib.vfb_format_infix.argtypes = [ctypes.POINTER(_Result), ctypes.POINTER(ctypes.c_char_p),
+                                     ctypes.c_char_p, ctypes.c_size_t]
+    lib.vfb_format_infix.restype = ctypes.c_int
+    _lib = lib
+    return lib
+
+
+# ------------------------------------------------------------------- problems
+@dataclass
+class Problem:
+    """Inputs in the reference's layout: words[i*num_vars + v], lengths[i]."""
+    num_vars: int
+    num_pos: int
+    words: list
+    lengths: list
+    names: list = field(default_factory=list)
+    max_size: int = MAX_SIZE
+    rlx_type: int = 3
+    max_length_traces: int = 0
+
+    @property
+    def num_traces(self) -> int:
+        return len(self.lengths)
+
+    @classmethod
+    def from_instance(cls, inst) -> "Problem":
+        """From a vfb_b200.synth.Instance."""
+        traces = inst.pos + inst.neg
+        words = [w[v] for _, w in traces for v in range(inst.num_vars)]
+        return cls(inst.num_vars, len(inst.pos), words, [l for l, _ in traces],
+                   list(inst.names) or [f"a{v}" for v in range(inst.num_vars)],
+                   inst.max_size, inst.rlx_type, max(l for l, _ in traces))
+
+    def _cstruct(self):
+        w = (ctypes.c_uint64 * max(1, len(self.words)))(*self.words)
+        ln = (ctypes.c_int * max(1, len(self.lengths)))(*self.lengths)
+        s = _Instance(self.num_vars, self.num_traces, self.num_pos,
+                      ctypes.cast(w, ctypes.POINTER(ctypes.c_uint64)),
+                      ctypes.cast(ln, ctypes.POINTER(ctypes.c_int)), self.max_size, self.rlx_type)
+        return s, (w, ln)
+
+
+@dataclass
+class Result:
+    status: int
+    size: int
+    rpn: list
+    level_rows: list
+    level_cands: list
+    total_rows: int
+    solution_index: int
+    seconds: float
+
+    @property
+    def found(self) -> bool:
+        return self.status == OK
+
+    def infix(self, names) -> str:
+        st = []
+        for tk in self.rpn:
+            if isinstance(tk, int):
+                st.append(names[tk])
+            elif tk in "~XFG":
+                st.append(f"{tk}({st.pop()})")
+            else:
+                r = st.pop()
+                l = st.pop()
+                st.append(f"({l}) {tk} ({r})")
+        return st[0] if len(st) == 1 else ""
+
+
+def _result(r: _Result) -> Result:
+    k = max(0, min(r.size, MAX_SIZE))
+    rpn = [r.rpn[i] if r.rpn[i] >= 0 else OPS[-r.rpn[i] - 1] for i in range(r.rpn_len)]
+    return Result(r.status, r.size, rpn, [r.level_rows[i] for i in range(1, k + 1)],
+                  [r.level_cands[i] for i in range(1, k + 1)], r.total_rows, r.solution_index,
+                  r.seconds)
+
+
+def read_json_file(path: str) -> Problem:
+    """Parse a trace file in the reference's JSON schema with the library's reader."""
+    lib = load_library()
+    out = ctypes.POINTER(_JsonProblem)()
+    err = ctypes.create_string_buffer(512)
+    rc = lib.vfb_read_json(path.encode(), ctypes.byref(out), err, len(err))
+    if rc != OK:
+        raise VfbError(err.value.decode() or STATUS_NAMES[rc])
+    try:
+        jp = out.contents
+        inst = jp.inst
+        t, a = inst.num_traces, inst.num_vars
+        words = [inst.words[i] for i in range(t * a)]
+        lengths = [inst.lengths[i] for i in range(t)]
+        names = [jp.names[v].decode() for v in range(a)]
+        return Problem(a, inst.num_pos, words, lengths, names, MAX_SIZE, 3, jp.max_length_traces)
+    finally:
+        lib.vfb_json_free(out)
+
+
+# --------------------------------------------------------------------- engine
+class Engine:
+    """One CUDA context/stream of the engine (vfb_create ... vfb_destroy)."""
+
+    def __init__(self, device: int = 0, mem_limit_bytes: int = 0, verbose: bool = False):
+        self._lib = load_library()
+        self._ctx = ctypes.c_void_p()
+        opts = _Opts(device, mem_limit_bytes, 1 if verbose else 0)
+        rc = self._lib.vfb_create(ctypes.byref(self._ctx), ctypes.byref(opts))
+        if rc != OK:
+            raise VfbError(f"vfb_create failed: {STATUS_NAMES[rc]} (a B200 and the sm_100a build "
+                           "are required; there is no CPU fallback)")
+
+    def close(self):
+        if self._ctx:
+            self._lib.vfb_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+    def solve(self, prob: Problem) -> Result:
+        inst, keep = prob._cstruct()
+        res = _Result()
+        self._lib.vfb_solve(self._ctx, ctypes.byref(inst), ctypes.byref(res))
+        del keep
+        return _result(res)
+
+    def batch_solve(self, probs: list) -> list:
+        n = len(probs)
+        if n == 0:
+            return []
+        arr = (_Instance * n)()
+        keep = []
+        for i, p in enumerate(probs):
+            s, k = p._cstruct()
+            arr[i] = s
+            keep.append(k)
+        res = (_Result * n)()
+        rc = self._lib.vfb_batch_solve(self._ctx, arr, n, res)
+        if rc not in (OK, NOT_FOUND):
+            raise VfbError(f"vfb_batch_solve failed: {STATUS_NAMES[rc]}")
+        return [_result(res[i]) for i in range(n)]
+
+
+def ltl(max_len: int, input_data, trace_len, num_vars: int, num_pos: int, names,
+        rlx_type: int = 3, engine: Engine | None = None) -> str:
+    """Same contract as the reference's LTL(): the smallest formula's infix text,
+    or "Not found !" when none exists up to max_len."""
+    eng = engine or Engine()
+    res = eng.solve(Problem(num_vars, num_pos, list(input_data), list(trace_len), list(names),
+                            max_len, rlx_type))
+    if res.status == OK:
+        return res.infix(names)
+    if res.status == NOT_FOUND:
+        return "Not found !"
+    raise VfbError(STATUS_NAMES[res.status])

@@ -1,0 +1,187 @@
+// vfb_device.cuh -- device-side data layout and per-word primitives.
+//
+// Characteristic set (CS): one uint64 word per trace, bit t = "formula holds
+// at step t of that trace" (LTL_BS.cu:146, 183-238).  Rows of the level cache
+// are stored row-major with a padded pitch of TP = T rounded up to an even
+// number of words, so every row starts on a 16-byte boundary (128-bit loads,
+// bulk copies).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace vfb {
+
+constexpr int kMaxTraces = 128;
+constexpr int kMaxSize = 32;          // formula size limit (ltl_nocache.cu:11)
+constexpr int kMaxSplits = 16;        // floor((32-1)/2)
+constexpr int kGroups = 1 + kMaxSplits;
+constexpr int kTS = 128;              // stream rows per P1 tile (= threads per CTA)
+constexpr int kTQ = 32;               // staged rows per P1 tile
+constexpr int kMaxProbes = 4096;      // bounded linear probing
+constexpr uint64_t kEmpty = ~0ULL;
+constexpr int kPayShift = 58;         // payload = level << 58 | candidate index
+constexpr uint64_t kIdxMask = (1ULL << kPayShift) - 1;
+
+enum Op : int { OP_NOT = 0, OP_AND, OP_OR, OP_X, OP_F, OP_G, OP_U, OP_ATOM = 7 };
+
+enum Status : int {
+  ST_IDLE = 0,
+  ST_RUNNING = 1,
+  ST_FOUND = 2,
+  ST_NOT_FOUND = 3,
+  ST_NEED_MEM = 4,     // a buffer is too small: host grows it and re-runs the level
+  ST_ERROR = 5,
+};
+
+enum NeedBits : int {
+  NEED_BITMAP = 1, NEED_TABLE = 2, NEED_TENT = 4, NEED_ROWS = 8, NEED_LIMIT = 16,
+};
+
+enum KeyMode : int { KEY_CONCAT = 0, KEY_SAMPLED = 1, KEY_HASH = 3 };
+
+struct __align__(32) Slot {
+  unsigned long long h, l, pay, aux;
+};
+struct __align__(16) Key128 {
+  unsigned long long h, l;
+};
+
+// Per-instance device state.  Kernels read everything they need from here,
+// so one captured launch sequence serves every level and every batch.
+struct InstDev {
+  // ---- problem (written once by the host)
+  int T, TP, A, npos, max_size, key_mode, stride1, lensum;
+  uint8_t len[kMaxTraces];
+  uint8_t off[kMaxTraces];     // bit offset of the trace's key field (<=126)
+  uint8_t width[kMaxTraces];   // key field width (0 when past bit 126)
+  uint64_t posmask[2];         // bit i: trace i is positive
+  // ---- buffers (host-owned allocations; pointers may change between levels)
+  uint64_t* rows;              // [row_cap][TP]
+  uint64_t* origin;            // [row_cap] candidate index within the row's level
+  uint64_t row_cap;
+  Slot* table;
+  uint64_t table_mask;         // capacity - 1 (power of two)
+  uint32_t* bitmap;            // tentative-winner bits, one per candidate
+  uint64_t bitmap_words;
+  uint64_t* tent;              // tentative candidate indices (ascending)
+  uint64_t* wins;              // winner candidate indices (ascending)
+  uint64_t tent_cap;
+  // ---- search state
+  int status, level, need, pad0;
+  uint64_t need_amount[4];     // requested bitmap words / slots / tentatives / rows
+  uint64_t lstart[kMaxSize + 2];
+  uint64_t lcount[kMaxSize + 2];
+  uint64_t lcands[kMaxSize + 2];
+  uint64_t keys;               // keys in the table
+  uint64_t cands;              // candidates of the level being built
+  uint64_t base_not, base_x, base_f, base_g;
+  uint64_t base_and[kMaxSplits + 1], base_or[kMaxSplits + 1];
+  uint64_t base_u[kMaxSize];
+  // P1 tile groups: group 0 = unary over level k-1, group s = split s
+  uint64_t grp_prefix[kGroups + 1];
+  uint32_t grp_qtiles[kGroups];
+  // per-level counters
+  unsigned long long n_tent, n_new, n_wins, probe_fail;
+  unsigned long long best_sol;  // min candidate index of a solution winner
+  // ---- result
+  int res_size, rpn_len;
+  int16_t rpn[kMaxSize];
+  uint64_t sol_index;
+};
+
+// ------------------------------------------------------------- word operators
+__device__ __forceinline__ uint64_t len_mask(int L) {
+  return L >= 64 ? ~0ULL : ((1ULL << L) - 1ULL);
+}
+
+// F: bit t set iff some bit >= t is set (suffix OR), i.e. every bit at or
+// below the most significant set bit.  Same function as the shift-doubling of
+// LTL_BS.cu:208-213, computed from the leading-zero count.
+__device__ __forceinline__ uint64_t w_fin(uint64_t w) {
+  const uint64_t m = ~0ULL >> (__clzll((long long)w) & 63);
+  return w ? m : 0ULL;
+}
+
+__device__ __forceinline__ uint64_t w_glob(uint64_t w, uint64_t lm) {
+  return w & ~w_fin(~w & lm);
+}
+
+// l U r on one word: U_t = r_t | (l_t & U_{t+1}).  Reversing the bit order
+// turns the recurrence into a carry chain (generate = r, propagate = l), which
+// one 64-bit addition resolves; the carry out of bit 63 supplies the top bit.
+// Equal to the 6-step doubling of LTL_BS.cu:222-233 on every input.
+__device__ __forceinline__ uint64_t w_until(uint64_t l, uint64_t r) {
+  const uint64_t lr = __brevll(l), rr = __brevll(r);
+  const uint64_t a = lr | rr;
+  const uint64_t s = a + rr;
+  const uint64_t c = s ^ a ^ rr;
+  const uint64_t cout = (s < a) ? 1ULL : 0ULL;
+  return __brevll((c >> 1) | (cout << 63));
+}
+
+__device__ __forceinline__ uint64_t splitmix_fin(uint64_t x) {
+  x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  x = (x ^ (x >> 27)) * 0x94d049bb133111ebULL;
+  return x ^ (x >> 31);
+}
+
+// ------------------------------------------------------------------ key state
+// Streaming accumulation of the 126-bit key of LTL_BS.cu:30-110 over the words
+// of one CS (word i of trace i, in trace order).
+struct KeyAcc {
+  uint64_t a0, a1;  // KEY_CONCAT/KEY_SAMPLED: bits 0..127; KEY_HASH: l, h
+};
+
+__device__ __forceinline__ void key_init(KeyAcc& k) { k.a0 = k.a1 = 0; }
+
+__device__ __forceinline__ uint64_t compress_stride(uint64_t w, int stride, int L) {
+  uint64_t f = 0;
+  int j = 0;
+  for (int k = 0; k < L; k += stride, ++j) f |= ((w >> k) & 1ULL) << j;
+  return f;
+}
+
+template <int MODE>
+__device__ __forceinline__ void key_word(KeyAcc& k, uint64_t w, int i, int half, int off, int width,
+                                         int stride, int L) {
+  if (MODE == KEY_HASH) {
+    const uint64_t x = splitmix_fin(w);
+    if (i < half) k.a1 ^= x; else k.a0 ^= x;   // a1 = h, a0 = l
+  } else {
+    uint64_t f = (MODE == KEY_SAMPLED) ? compress_stride(w, stride, L) : w;
+    f &= (width >= 64) ? ~0ULL : ((1ULL << width) - 1ULL);
+    if (width == 0) return;
+    if (off < 64) {
+      k.a0 |= f << off;
+      if (off > 0 && off + width > 64) k.a1 |= f >> (64 - off);
+    } else {
+      k.a1 |= f << (off - 64);
+    }
+  }
+}
+
+template <int MODE>
+__device__ __forceinline__ void key_final(const KeyAcc& k, uint64_t& h, uint64_t& l) {
+  if (MODE == KEY_HASH) {
+    h = k.a1;
+    l = k.a0;
+  } else {
+    const uint64_t lo = k.a0, hi = k.a1 & ((1ULL << 62) - 1ULL);   // 126 bits
+    l = lo & ((1ULL << 63) - 1ULL);
+    h = ((lo >> 63) | (hi << 1)) & ((1ULL << 63) - 1ULL);
+  }
+  // WarpCore rejects its empty (~0) and tombstone (~0-1) keys with slot code 0
+  // (hash_set.cuh:201-205): both values name the same pair component.
+  if (h == ~0ULL) h = ~0ULL - 1;
+  if (l == ~0ULL) l = ~0ULL - 1;
+}
+
+__device__ __forceinline__ uint64_t slot_hash(uint64_t h, uint64_t l) {
+  return splitmix_fin(h ^ (l * 0x9E3779B97F4A7C15ULL) ^ 0x5ad0dedULL);
+}
+
+__device__ __forceinline__ bool is_pos(const InstDev& I, int i) {
+  return (I.posmask[i >> 6] >> (i & 63)) & 1ULL;
+}
+
+}  // namespace vfb

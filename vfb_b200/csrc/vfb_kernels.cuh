@@ -1,0 +1,44 @@
+// vfb_kernels.cuh -- kernel entry points of the level step (see vfb_kernels.cu).
+#pragma once
+#include "vfb_device.cuh"
+
+namespace vfb {
+
+constexpr int kChunkWords = 4096;     // bitmap words per compaction chunk (131072 bits)
+constexpr int kChunkThreads = 256;    // threads per compaction CTA (16 words each)
+constexpr int kScanThreads = 1024;
+
+// Global batch descriptor, resident in device memory so that buffer growth
+// never invalidates a captured launch sequence.
+struct BatchDev {
+  InstDev* inst;
+  int ninst;
+  int pad;
+  unsigned long long* p1_prefix;        // [ninst+1] P1 tiles
+  unsigned long long* chunk_prefix0;    // [ninst+1] candidate-bitmap chunks
+  unsigned long long* chunk_prefix1;    // [ninst+1] winner-bitmap chunks
+  unsigned long long* tent_prefix;      // [ninst+1]
+  unsigned long long* win_prefix;       // [ninst+1]
+  unsigned int* chunk_cnt;              // [chunk_cap]
+  unsigned long long* chunk_base;       // [chunk_cap]
+  unsigned long long chunk_cap;
+  unsigned long long* tickets;          // [4]: P1 work ticket, scan0/scan1 done counters
+  int2* status_out;                     // [ninst] (status, need) mirror for the host
+};
+
+// Level-step kernels, launched in this order for every level.
+__global__ void k_plan(BatchDev* B);
+__global__ void k_p1(BatchDev* B);
+__global__ void k_chunk_count(BatchDev* B, int phase);
+__global__ void k_chunk_scan(BatchDev* B, int phase);
+__global__ void k_chunk_emit(BatchDev* B, int phase);
+__global__ void k_verify(BatchDev* B);
+__global__ void k_emit_rows(BatchDev* B);
+__global__ void k_finish(BatchDev* B);
+
+// Set-up and maintenance kernels.
+__global__ void k_init(BatchDev* B);
+__global__ void k_rehash(const Slot* old_tab, unsigned long long old_cap, Slot* new_tab,
+                         unsigned long long new_mask, unsigned long long* fail);
+
+}  // namespace vfb

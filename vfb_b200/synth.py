@@ -1,0 +1,341 @@
+"""Seeded synthetic LTL-learning instances (trace samples) in VFB's JSON schema.
+
+The reference ships no benchmark inputs (its one example, ExampleLTLF.json, has
+no pinned answer), so the workloads are generated here from a portable RNG:
+splitmix64 seeds a xoshiro256** stream, so the same seed gives the same traces
+on every machine and in every language that restates the two generators.
+
+Planted formulas are drawn uniformly over all formulas of a given size with the
+formula numbering of ltl_nocache.cu (generateMatrix ltl_nocache.cu:248-287,
+numberToFormula ltl_nocache.cu:169-224): a number n < numForm[size][7] is drawn
+uniformly and decoded to RPN.  Traces are labelled by evaluating the planted
+formula at step 0 with the operator semantics of ltl_nocache.cu:95-150.
+
+Trace JSON follows ltl_nocache.cu:46-73 (keys number_atomic_propositions,
+number_traces, number_positive_traces, max_length_traces, atomic_propositions,
+positive_traces[], negative_traces[] with one 0/1 array per proposition).
+"""
+from __future__ import annotations
+
+import json
+import math
+from dataclasses import dataclass, field
+
+M64 = (1 << 64) - 1
+OPS = "~&|XFGU"          # operator order of the reference (Op enum LTL_BS.cu:17)
+UNARY = set("~XFG")
+
+
+# --------------------------------------------------------------------------- RNG
+def splitmix64(state: int):
+    state = (state + 0x9E3779B97F4A7C15) & M64
+    z = state
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M64
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M64
+    return state, z ^ (z >> 31)
+
+
+def _rotl(x: int, k: int) -> int:
+    return ((x << k) | (x >> (64 - k))) & M64
+
+
+class Rng:
+    """xoshiro256** seeded by four splitmix64 outputs."""
+
+    def __init__(self, seed: int):
+        st = seed & M64
+        self.s = []
+        for _ in range(4):
+            st, z = splitmix64(st)
+            self.s.append(z)
+
+    def next_u64(self) -> int:
+        s = self.s
+        result = (_rotl((s[1] * 5) & M64, 7) * 9) & M64
+        t = (s[1] << 17) & M64
+        s[2] ^= s[0]
+        s[3] ^= s[1]
+        s[1] ^= s[2]
+        s[0] ^= s[3]
+        s[2] ^= t
+        s[3] = _rotl(s[3], 45)
+        return result
+
+    def below(self, n: int) -> int:
+        """Uniform integer in [0, n) by rejection (n may exceed 2^64)."""
+        if n <= 0:
+            raise ValueError("empty range")
+        bits = max(1, (n - 1).bit_length())
+        words = (bits + 63) // 64
+        while True:
+            v = 0
+            for _ in range(words):
+                v = (v << 64) | self.next_u64()
+            v >>= words * 64 - bits
+            if v < n:
+                return v
+
+    def uniform_int(self, lo: int, hi: int) -> int:
+        """Uniform integer in [lo, hi] inclusive."""
+        return lo + self.below(hi - lo + 1)
+
+    def random(self) -> float:
+        return (self.next_u64() >> 11) * (1.0 / (1 << 53))
+
+    def bernoulli_word(self, nbits: int, p: float) -> int:
+        w = 0
+        for t in range(nbits):
+            if self.random() < p:
+                w |= 1 << t
+        return w
+
+
+# ------------------------------------------------------------ formula numbering
+def formula_counts(num_vars: int, max_len: int) -> list[list[int]]:
+    """numForm[size][op] / numForm[size][7] (ltl_nocache.cu:248-287)."""
+    n = [[0] * 8 for _ in range(max(max_len, 2) + 1)]
+    n[1][7] = num_vars
+    for o in (0, 3, 4, 5):
+        n[2][o] = num_vars
+    n[2][7] = 4 * num_vars
+    for i in range(3, max_len + 1):
+        un = n[i - 1][7]
+        com = sum(n[j][7] * n[i - j - 1][7] for j in range(1, (i - 1) // 2 + 1))
+        ncom = sum(n[j][7] * n[i - j - 1][7] for j in range(1, i - 1))
+        n[i][0] = n[i][3] = n[i][4] = n[i][5] = un
+        n[i][1] = n[i][2] = com
+        n[i][6] = ncom
+        n[i][7] = 4 * un + 2 * com + ncom
+    return n
+
+
+def number_to_rpn(n: int, size: int, counts) -> list:
+    """Decode formula number n of the given size into RPN tokens.
+
+    Tokens are ints (proposition index) or operator characters.  Mirrors the
+    numbering of numberToFormula (ltl_nocache.cu:169-224): operator blocks in
+    the order ~ & | X F G U, binary operands split by left size ascending, left
+    formula number major, right minor.
+    """
+    if size == 1:
+        return [n]
+    op = 0
+    while n >= counts[size][op]:
+        n -= counts[size][op]
+        op += 1
+    ch = OPS[op]
+    sub = size - 1
+    if ch in UNARY:
+        return number_to_rpn(n, sub, counts) + [ch]
+    left = 1
+    while n >= counts[left][7] * counts[sub - left][7]:
+        n -= counts[left][7] * counts[sub - left][7]
+        left += 1
+    nr = counts[sub - left][7]
+    return (number_to_rpn(n // nr, left, counts)
+            + number_to_rpn(n % nr, sub - left, counts) + [ch])
+
+
+def _mask(length: int) -> int:
+    return M64 if length >= 64 else (1 << length) - 1
+
+
+def _suffix_or(w: int) -> int:
+    for s in (1, 2, 4, 8, 16, 32):
+        w |= w >> s
+    return w
+
+
+def eval_rpn_word(rpn, words, length: int) -> int:
+    """Characteristic word of an RPN formula on one trace (bit t = holds at t).
+
+    words[v] is proposition v's word on this trace.  Semantics of
+    ltl_nocache.cu:95-150.
+    """
+    st = []
+    m = _mask(length)
+    for tok in rpn:
+        if isinstance(tok, int):
+            st.append(words[tok])
+        elif tok == "~":
+            st.append(~st.pop() & m)
+        elif tok == "X":
+            st.append(st.pop() >> 1)
+        elif tok == "F":
+            st.append(_suffix_or(st.pop()))
+        elif tok == "G":
+            x = st.pop()
+            st.append(x & ~_suffix_or(~x & m) & M64)
+        else:
+            r = st.pop()
+            l = st.pop()
+            if tok == "&":
+                st.append(l & r)
+            elif tok == "|":
+                st.append(l | r)
+            else:  # U
+                for s in (1, 2, 4, 8, 16):
+                    r |= l & (r >> s)
+                    l &= l >> s
+                r |= l & (r >> 32)
+                st.append(r)
+    assert len(st) == 1
+    return st[0]
+
+
+def rpn_to_infix(rpn, names) -> str:
+    """Infix printing of ltl_nocache.cu:289-317."""
+    st = []
+    for tok in rpn:
+        if isinstance(tok, int):
+            st.append(names[tok])
+        elif tok in UNARY:
+            st.append(f"{tok}({st.pop()})")
+        else:
+            r = st.pop()
+            l = st.pop()
+            st.append(f"({l}) {tok} ({r})")
+    return st[0]
+
+
+# -------------------------------------------------------------------- instances
+@dataclass
+class Instance:
+    """One learning problem: traces are lists of per-proposition words."""
+    num_vars: int
+    pos: list            # list of (length, [word per var])
+    neg: list
+    max_size: int
+    names: list = field(default_factory=list)
+    planted: list | None = None
+    rlx_type: int = 3
+    name: str = ""
+
+    @property
+    def num_traces(self) -> int:
+        return len(self.pos) + len(self.neg)
+
+    def lengths(self) -> list[int]:
+        return [l for l, _ in self.pos] + [l for l, _ in self.neg]
+
+    def atom_words(self) -> list[list[int]]:
+        """atoms[v][i]: proposition v's word on trace i (positives first)."""
+        traces = self.pos + self.neg
+        return [[w[v] for _, w in traces] for v in range(self.num_vars)]
+
+    def to_json(self) -> dict:
+        names = self.names or [f"a{v}" for v in range(self.num_vars)]
+
+        def tr(length, words):
+            return {names[v]: [(words[v] >> t) & 1 for t in range(length)]
+                    for v in range(self.num_vars)}
+
+        d = {
+            "number_atomic_propositions": self.num_vars,
+            "number_traces": self.num_traces,
+            "number_positive_traces": len(self.pos),
+            "number_negative_traces": len(self.neg),
+            "max_length_traces": max(self.lengths()) if self.num_traces else 0,
+            "atomic_propositions": names,
+            "positive_traces": [tr(l, w) for l, w in self.pos],
+            "negative_traces": [tr(l, w) for l, w in self.neg],
+        }
+        if self.planted is not None:
+            d["generating_formula"] = rpn_to_infix(self.planted, names)
+        return d
+
+    def write_json(self, path: str) -> None:
+        with open(path, "w") as f:
+            json.dump(self.to_json(), f)
+
+
+def _random_trace(rng: Rng, num_vars: int, length: int, p: float):
+    return (length, [rng.bernoulli_word(length, p) for _ in range(num_vars)])
+
+
+def planted_instance(rng: Rng, num_vars: int, planted_size: int, n_pos: int,
+                     n_neg: int, length_fn, p: float, max_size: int,
+                     max_draws_per_trace: int = 400, name: str = "") -> Instance:
+    """Rejection-sample traces labelled by a uniformly drawn planted formula.
+
+    A formula whose positive or negative class cannot be filled within
+    max_draws_per_trace * (n_pos + n_neg) draws is redrawn.
+    """
+    counts = formula_counts(num_vars, planted_size)
+    while True:
+        rpn = number_to_rpn(rng.below(counts[planted_size][7]), planted_size, counts)
+        pos, neg = [], []
+        budget = max_draws_per_trace * (n_pos + n_neg)
+        while (len(pos) < n_pos or len(neg) < n_neg) and budget > 0:
+            budget -= 1
+            length, words = _random_trace(rng, num_vars, length_fn(), p)
+            holds = eval_rpn_word(rpn, words, length) & 1
+            if holds and len(pos) < n_pos:
+                pos.append((length, words))
+            elif not holds and len(neg) < n_neg:
+                neg.append((length, words))
+        if len(pos) == n_pos and len(neg) == n_neg:
+            return Instance(num_vars, pos, neg, max_size,
+                            [f"a{v}" for v in range(num_vars)], rpn, 3, name)
+
+
+def config_small(seed: int = 0) -> Instance:
+    """Plain method, small: 2 APs, 1 pos + 2 neg traces of length 4, max size 10."""
+    rng = Rng(seed)
+    while True:
+        pos = [_random_trace(rng, 2, 4, 0.5)]
+        neg = [_random_trace(rng, 2, 4, 0.5) for _ in range(2)]
+        if all(n != pos[0] for n in neg):
+            return Instance(2, pos, neg, 10, ["a0", "a1"], None, 3, "small")
+
+
+def config_planted(seed: int = 1) -> Instance:
+    """Planted single instance: 4 APs, size-9 planted formula, 20+20 traces of length 16."""
+    rng = Rng(seed)
+    return planted_instance(rng, 4, 9, 20, 20, lambda: 16, 0.5, 13, name="planted")
+
+
+def config_large(seed: int = 2, length: int = 64, planted_size: int = 13,
+                 max_size: int = 17) -> Instance:
+    """Planted large instance: 8 APs, 31 pos + 32 neg traces of length 64, p=0.3."""
+    rng = Rng(seed)
+    return planted_instance(rng, 8, planted_size, 31, 32, lambda: length, 0.3,
+                            max_size, name="large")
+
+
+def batch_instance(rng: Rng, idx: int = 0) -> Instance:
+    """One instance of the mixed batch: A~U{2..8}, T~U{4..63}, L~U{4..64} per trace."""
+    a = rng.uniform_int(2, 8)
+    t = rng.uniform_int(4, 63)
+    n_pos = t // 2 if rng.below(2) == 0 else (t + 1) // 2
+    size = rng.uniform_int(5, 11)
+    return planted_instance(rng, a, size, n_pos, t - n_pos,
+                            lambda: rng.uniform_int(4, 64), 0.5, size + 4,
+                            name=f"batch{idx}")
+
+
+def config_batch(seed: int = 3, count: int = 256) -> list[Instance]:
+    rng = Rng(seed)
+    return [batch_instance(rng, i) for i in range(count)]
+
+
+def config_serving(seed: int = 4, count: int = 2000, rate: float = 100.0,
+                   large_frac: float = 0.05, large_fn=None):
+    """Poisson request stream: (arrival_time_s, Instance) pairs.
+
+    95% of requests are drawn like the mixed batch, 5% like the large instance
+    (large_fn builds those; default: config_large shape with a per-request seed).
+    """
+    rng = Rng(seed)
+    t = 0.0
+    out = []
+    for i in range(count):
+        u = rng.random()
+        t += -math.log(1.0 - u) / rate
+        if rng.random() < large_frac:
+            s = rng.next_u64()
+            inst = (large_fn or (lambda sd: config_large(sd)))(s)
+        else:
+            inst = batch_instance(rng, i)
+        out.append((t, inst))
+    return out
