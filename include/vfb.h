@@ -56,6 +56,8 @@ typedef struct {
   int device;              /* CUDA device ordinal */
   size_t mem_limit_bytes;  /* device memory budget of one solve/batch (0: 90% of free memory) */
   int verbose;             /* 1: per-level progress lines on stderr */
+  int profile;             /* 1: time every kernel of the level step with CUDA events
+                              (see vfb_profile_read); adds one event pair per kernel */
 } vfb_opts;
 
 /* One learning problem.  Layout as ltl_nocache's readJsonFile: words[i*num_vars + v]
@@ -84,6 +86,10 @@ typedef struct {
   uint64_t total_rows;               /* sum of level_rows */
   uint64_t solution_index;           /* canonical index of the solution within its size */
   double seconds;                    /* wall time of the call (batch: of the whole batch) */
+  double device_seconds;             /* device timeline from the first upload to the last
+                                        result read (CUDA events on the engine's stream) */
+  uint64_t h2d_bytes, d2h_bytes;     /* bytes copied host->device / device->host by the call */
+  uint64_t kernel_launches;          /* kernels this call launched */
 } vfb_result;
 
 vfb_status vfb_create(void **ctx, const vfb_opts *opts);
@@ -93,6 +99,21 @@ vfb_status vfb_solve(void *ctx, const vfb_instance *inst, vfb_result *out);
 
 /* Solves n independent instances together; out[i] equals vfb_solve(inst[i]). */
 vfb_status vfb_batch_solve(void *ctx, const vfb_instance *inst, int n, vfb_result *out);
+
+/* Per-kernel profile accumulated since vfb_create (profile=1 only).  name,
+ * number of launches, total device milliseconds (CUDA events around each
+ * launch) and the algorithmic bytes those launches had to move (operand rows
+ * read once, one 32-byte slot sector per hash probe, rows and indices written,
+ * bitmap words).  Returns the number of kernels written (at most cap). */
+typedef struct {
+  char name[32];
+  uint64_t launches;
+  double ms;
+  double bytes;
+} vfb_kernel_stat;
+
+int vfb_profile_read(void *ctx, vfb_kernel_stat *out, int cap);
+void vfb_profile_reset(void *ctx);
 
 /* Human-readable name of a status. */
 const char *vfb_status_str(vfb_status s);

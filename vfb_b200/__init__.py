@@ -35,7 +35,7 @@ class VfbError(RuntimeError):
 
 class _Opts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("mem_limit_bytes", ctypes.c_size_t),
-                ("verbose", ctypes.c_int)]
+                ("verbose", ctypes.c_int), ("profile", ctypes.c_int)]
 
 
 class _Instance(ctypes.Structure):
@@ -51,7 +51,14 @@ class _Result(ctypes.Structure):
                 ("level_rows", ctypes.c_uint64 * (MAX_SIZE + 1)),
                 ("level_cands", ctypes.c_uint64 * (MAX_SIZE + 1)),
                 ("total_rows", ctypes.c_uint64), ("solution_index", ctypes.c_uint64),
-                ("seconds", ctypes.c_double)]
+                ("seconds", ctypes.c_double), ("device_seconds", ctypes.c_double),
+                ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
+                ("kernel_launches", ctypes.c_uint64)]
+
+
+class _KernelStat(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 32), ("launches", ctypes.c_uint64),
+                ("ms", ctypes.c_double), ("bytes", ctypes.c_double)]
 
 
 class _JsonProblem(ctypes.Structure):
@@ -60,7 +67,8 @@ class _JsonProblem(ctypes.Structure):
 
 
 EXPORTS = ["vfb_create", "vfb_destroy", "vfb_solve", "vfb_batch_solve", "vfb_status_str",
-           "vfb_read_json", "vfb_json_free", "vfb_format_infix"]
+           "vfb_read_json", "vfb_json_free", "vfb_format_infix", "vfb_profile_read",
+           "vfb_profile_reset"]
 
 _lib = None
 
@@ -96,6 +104,10 @@ def load_library():
     lib.vfb_format_infix.argtypes = [ctypes.POINTER(_Result), ctypes.POINTER(ctypes.c_char_p),
                                      ctypes.c_char_p, ctypes.c_size_t]
     lib.vfb_format_infix.restype = ctypes.c_int
+    lib.vfb_profile_read.argtypes = [ctypes.c_void_p, ctypes.POINTER(_KernelStat), ctypes.c_int]
+    lib.vfb_profile_read.restype = ctypes.c_int
+    lib.vfb_profile_reset.argtypes = [ctypes.c_void_p]
+    lib.vfb_profile_reset.restype = None
     _lib = lib
     return lib
 
@@ -145,6 +157,10 @@ class Result:
     total_rows: int
     solution_index: int
     seconds: float
+    device_seconds: float = 0.0
+    h2d_bytes: int = 0
+    d2h_bytes: int = 0
+    kernel_launches: int = 0
 
     @property
     def found(self) -> bool:
@@ -169,7 +185,7 @@ def _result(r: _Result) -> Result:
     rpn = [r.rpn[i] if r.rpn[i] >= 0 else OPS[-r.rpn[i] - 1] for i in range(r.rpn_len)]
     return Result(r.status, r.size, rpn, [r.level_rows[i] for i in range(1, k + 1)],
                   [r.level_cands[i] for i in range(1, k + 1)], r.total_rows, r.solution_index,
-                  r.seconds)
+                  r.seconds, r.device_seconds, r.h2d_bytes, r.d2h_bytes, r.kernel_launches)
 
 
 def read_json_file(path: str) -> Problem:
@@ -196,10 +212,11 @@ def read_json_file(path: str) -> Problem:
 class Engine:
     """One CUDA context/stream of the engine (vfb_create ... vfb_destroy)."""
 
-    def __init__(self, device: int = 0, mem_limit_bytes: int = 0, verbose: bool = False):
+    def __init__(self, device: int = 0, mem_limit_bytes: int = 0, verbose: bool = False,
+                 profile: bool = False):
         self._lib = load_library()
         self._ctx = ctypes.c_void_p()
-        opts = _Opts(device, mem_limit_bytes, 1 if verbose else 0)
+        opts = _Opts(device, mem_limit_bytes, 1 if verbose else 0, 1 if profile else 0)
         rc = self._lib.vfb_create(ctypes.byref(self._ctx), ctypes.byref(opts))
         if rc != OK:
             raise VfbError(f"vfb_create failed: {STATUS_NAMES[rc]} (a B200 and the sm_100a build "
@@ -221,6 +238,15 @@ class Engine:
             self.close()
         except Exception:  # noqa: BLE001
             pass
+
+    def profile(self) -> list:
+        """Per-kernel (name, launches, total ms, algorithmic bytes) since creation."""
+        arr = (_KernelStat * 32)()
+        m = self._lib.vfb_profile_read(self._ctx, arr, 32)
+        return [(arr[i].name.decode(), arr[i].launches, arr[i].ms, arr[i].bytes) for i in range(m)]
+
+    def profile_reset(self) -> None:
+        self._lib.vfb_profile_reset(self._ctx)
 
     def solve(self, prob: Problem) -> Result:
         inst, keep = prob._cstruct()

@@ -4,15 +4,21 @@
 // The reference drives one launch per (level, operator, size split, chunk)
 // with a blocking device-to-host copy after each (LTL_BS.cu:1226-1488).  Here
 // a whole level of every instance in flight is one fixed launch sequence
-// (vfb_kernels.cu), captured once as a CUDA graph; the host only reads a
-// per-instance (status, need) word after each level and grows a buffer when
-// a kernel asked for more room.  All buffers come from the device's
-// stream-ordered memory pool, which keeps freed memory for the next solve.
+// (vfb_kernels.cu) that reads its work from device memory.  That sequence is
+// captured once as the body of a CUDA-graph while-node: the device keeps
+// building levels until every instance is solved, exhausted or needs a larger
+// buffer, so a solve is one graph launch and one status read.  The host only
+// steps in to grow a buffer (the level is then re-run; every kernel of the
+// step is idempotent) and to read the results.  Device buffers come from a
+// block cache on top of the stream-ordered pool, so repeated solves neither
+// allocate nor re-grow.
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <new>
 #include <vector>
 
@@ -25,9 +31,9 @@ namespace {
 
 struct InstHost {
   InstDev d;        // host copy of the device record
-  size_t bytes = 0; // device bytes held by this instance
   bool active = false;
   vfb_status fail = VFB_OK;
+  int accounted = 1;  // last level whose bytes were added to the profile
 };
 
 uint64_t pow2_at_least(uint64_t x) {
@@ -35,20 +41,40 @@ uint64_t pow2_at_least(uint64_t x) {
   while (p < x) p <<= 1;
   return p;
 }
+uint64_t pow2_at_most(uint64_t x) {
+  uint64_t p = 1;
+  while (2 * p <= x) p <<= 1;
+  return p;
+}
+
+// Kernels of one level step, in launch order (ids index Engine::prof).
+enum KId { KP_PLAN, KP_P1, KP_COUNT, KP_SCAN, KP_EMIT, KP_VERIFY, KP_ROWS, KP_FINISH, KP_LOOP, KP_INIT, KP_REHASH,
+           KP_N };
+const char* const kNames[KP_N] = {"k_plan", "k_p1", "k_chunk_count", "k_chunk_scan", "k_chunk_emit", "k_verify",
+                                  "k_emit_rows", "k_finish", "k_loop_ctl", "k_init", "k_rehash"};
+const int kStepSeq[] = {KP_PLAN, KP_P1, KP_COUNT, KP_SCAN, KP_EMIT, KP_VERIFY, KP_COUNT, KP_SCAN, KP_EMIT,
+                        KP_ROWS, KP_FINISH};
+constexpr int kStepLen = sizeof(kStepSeq) / sizeof(int);
+constexpr unsigned kMaxLoop = 4 * kMaxSize;
+
+struct Prof {
+  uint64_t launches = 0;
+  double ms = 0, bytes = 0;
+};
 
 }  // namespace
 
 struct Engine {
   int device = 0;
   int verbose = 0;
+  int profile = 0;
   size_t mem_limit = 0;
   cudaStream_t stream = nullptr;
-  cudaMemPool_t pool = nullptr;
   int sms = 0;
   int grid = 0;        // grid-stride CTAs (256 threads)
   int p1_grid = 0;     // P1 CTAs
-  int p1_smem_max = 0;
   cudaError_t last_error = cudaSuccess;
+  bool use_loop = true;  // device-side while-node available
 
   // batch workspace
   int ninst_cap = 0;
@@ -57,56 +83,102 @@ struct Engine {
   InstDev* dInst = nullptr;
   int2* h_status = nullptr;   // pinned mirror of B.status_out
   unsigned long long* d_fail = nullptr;
+  uint64_t* h_stage = nullptr;  // pinned upload staging
+  size_t h_stage_words = 0;
 
-  // graph of one level step
-  cudaGraphExec_t step_exec = nullptr;
-  int step_ninst = -1, step_smem = -1, step_grid = -1;
+  // graphs
+  cudaGraphExec_t exec = nullptr;
+  int exec_ninst = -1, exec_smem = -1, exec_grid = -1, exec_loop = -1;
 
-  size_t used_bytes = 0;
+  // device block cache: size -> blocks
+  std::multimap<size_t, void*> free_blocks;
+  std::map<void*, size_t> live_blocks;
+  size_t held_bytes = 0;  // live + cached
+
+  // per-call counters
+  uint64_t c_h2d = 0, c_d2h = 0, c_launch = 0;
+  cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr;
+  cudaEvent_t ev_k[kStepLen + 1] = {};
+  Prof prof[KP_N];
 
   ~Engine() { release(); }
 
   void release() {
-    if (step_exec) cudaGraphExecDestroy(step_exec);
-    step_exec = nullptr;
+    if (stream) cudaStreamSynchronize(stream);
+    if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
     free_workspace();
+    for (auto& kv : free_blocks) cudaFree(kv.second);
+    free_blocks.clear();
+    for (auto& kv : live_blocks) cudaFree(kv.first);
+    live_blocks.clear();
     if (h_status) cudaFreeHost(h_status);
     h_status = nullptr;
+    if (h_stage) cudaFreeHost(h_stage);
+    h_stage = nullptr;
     if (d_fail) cudaFree(d_fail);
     d_fail = nullptr;
+    if (ev_t0) cudaEventDestroy(ev_t0);
+    if (ev_t1) cudaEventDestroy(ev_t1);
+    for (auto& e : ev_k)
+      if (e) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
     stream = nullptr;
   }
 
   void free_workspace() {
-    auto f = [&](void* p) { if (p) cudaFreeAsync(p, stream); };
+    auto f = [&](void* p) { if (p) cudaFree(p); };
     f(hB.p1_prefix); f(hB.chunk_prefix0); f(hB.chunk_prefix1); f(hB.tent_prefix); f(hB.win_prefix);
-    f(hB.chunk_cnt); f(hB.chunk_base); f(hB.tickets); f(hB.status_out); f(dB); f(dInst);
+    f(hB.chunk_cnt); f(hB.chunk_base); f(hB.tickets); f(hB.status_out); f(hB.loop_iter); f(dB); f(dInst);
     hB = BatchDev{};
     dB = nullptr;
     dInst = nullptr;
     ninst_cap = 0;
-    if (stream) cudaStreamSynchronize(stream);
   }
 
-  cudaError_t dalloc(void** p, size_t bytes) {
-    *p = nullptr;
-    if (bytes == 0) bytes = 16;
-    if (mem_limit && used_bytes + bytes > mem_limit) return cudaErrorMemoryAllocation;
-    cudaError_t e = cudaMallocAsync(p, bytes, stream);
-    if (e == cudaSuccess) used_bytes += bytes;
-    return e;
-  }
-  void dfree(void* p, size_t bytes) {
-    if (p) {
-      cudaFreeAsync(p, stream);
-      used_bytes -= std::min(used_bytes, bytes);
+  // ------------------------------------------------------ device blocks
+  // Returns a block of at least `bytes`; *got is its real size.  Cached blocks
+  // up to 4x the request are reused (their full size becomes the capacity).
+  void* dalloc(size_t bytes, size_t* got) {
+    if (bytes < 256) bytes = 256;
+    auto it = free_blocks.lower_bound(bytes);
+    if (it != free_blocks.end() && it->first <= 4 * bytes) {
+      void* p = it->second;
+      *got = it->first;
+      free_blocks.erase(it);
+      live_blocks[p] = *got;
+      return p;
     }
+    // make room: drop cached blocks before exceeding the budget
+    while (mem_limit && held_bytes + bytes > mem_limit && !free_blocks.empty()) {
+      auto big = std::prev(free_blocks.end());
+      cudaFreeAsync(big->second, stream);
+      held_bytes -= big->first;
+      free_blocks.erase(big);
+    }
+    if (mem_limit && held_bytes + bytes > mem_limit) return nullptr;
+    void* p = nullptr;
+    if (cudaMallocAsync(&p, bytes, stream) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    held_bytes += bytes;
+    live_blocks[p] = bytes;
+    *got = bytes;
+    return p;
+  }
+  void dfree(void* p) {
+    if (!p) return;
+    auto it = live_blocks.find(p);
+    if (it == live_blocks.end()) return;
+    free_blocks.emplace(it->second, p);
+    live_blocks.erase(it);
   }
 
   vfb_status init(const vfb_opts* o) {
     device = o ? o->device : 0;
     verbose = o ? o->verbose : 0;
+    profile = o ? o->profile : 0;
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n <= device) return VFB_DEVICE_ERROR;
     if (cudaSetDevice(device) != cudaSuccess) return VFB_DEVICE_ERROR;
@@ -122,33 +194,37 @@ struct Engine {
     cudaMemGetInfo(&freeb, &total);
     mem_limit = (o && o->mem_limit_bytes) ? o->mem_limit_bytes : (size_t)(0.9 * (double)freeb);
     if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) return VFB_DEVICE_ERROR;
+    cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
       uint64_t thr = ~0ULL;
       cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
     }
     if (cudaMalloc(&d_fail, sizeof(unsigned long long)) != cudaSuccess) return VFB_DEVICE_ERROR;
+    if (cudaEventCreate(&ev_t0) != cudaSuccess || cudaEventCreate(&ev_t1) != cudaSuccess) return VFB_DEVICE_ERROR;
+    for (auto& e : ev_k)
+      if (cudaEventCreate(&e) != cudaSuccess) return VFB_DEVICE_ERROR;
     grid = sms * 8;
-    p1_smem_max = 0;
-    // P1 must be able to hold the largest staged tile (128 traces)
     const int maxsmem = (kTS * (kMaxTraces + 1) + kTQ * kMaxTraces) * 8;
     if (cudaFuncSetAttribute(k_p1, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsmem) != cudaSuccess)
       return VFB_DEVICE_ERROR;
-    // a quick launch of a trivial kernel proves the image runs on this device
-    if (cudaFuncGetAttributes(&fattr_, k_p1) != cudaSuccess) return VFB_DEVICE_ERROR;
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, k_p1) != cudaSuccess) return VFB_DEVICE_ERROR;
+    const char* env = std::getenv("VFB_NO_DEVICE_LOOP");
+    use_loop = !(env && env[0] == '1') && !profile;
     return VFB_OK;
   }
-  cudaFuncAttributes fattr_{};
 
   // ------------------------------------------------------------ workspace
   vfb_status ensure_workspace(int ninst, uint64_t chunk_need) {
     if (ninst > ninst_cap || chunk_need > hB.chunk_cap) {
+      if (cudaStreamSynchronize(stream) != cudaSuccess) return VFB_DEVICE_ERROR;
       const int nc = std::max(ninst, ninst_cap);
       const uint64_t cc = std::max<uint64_t>(chunk_need, hB.chunk_cap);
       BatchDev nb{};
       void* p = nullptr;
       const size_t pre = (size_t)(nc + 1) * sizeof(unsigned long long);
-#define WS_ALLOC(field, bytes)                                            \
-  if (cudaMallocAsync(&p, (bytes), stream) != cudaSuccess) return VFB_OOM; \
+#define WS_ALLOC(field, bytes)                               \
+  if (cudaMalloc(&p, (bytes)) != cudaSuccess) return VFB_OOM; \
   nb.field = reinterpret_cast<decltype(nb.field)>(p);
       WS_ALLOC(p1_prefix, pre)
       WS_ALLOC(chunk_prefix0, pre)
@@ -159,14 +235,15 @@ struct Engine {
       WS_ALLOC(chunk_base, std::max<uint64_t>(cc, 1) * sizeof(unsigned long long))
       WS_ALLOC(tickets, 4 * sizeof(unsigned long long))
       WS_ALLOC(status_out, (size_t)nc * sizeof(int2))
+      WS_ALLOC(loop_iter, sizeof(unsigned long long))
 #undef WS_ALLOC
       BatchDev* ndB = nullptr;
-      if (cudaMallocAsync((void**)&ndB, sizeof(BatchDev), stream) != cudaSuccess) return VFB_OOM;
+      if (cudaMalloc((void**)&ndB, sizeof(BatchDev)) != cudaSuccess) return VFB_OOM;
       InstDev* ndI = nullptr;
-      if (cudaMallocAsync((void**)&ndI, (size_t)nc * sizeof(InstDev), stream) != cudaSuccess) return VFB_OOM;
+      if (cudaMalloc((void**)&ndI, (size_t)nc * sizeof(InstDev)) != cudaSuccess) return VFB_OOM;
       if (dInst && ninst_cap)
-        cudaMemcpyAsync(ndI, dInst, (size_t)ninst_cap * sizeof(InstDev), cudaMemcpyDeviceToDevice, stream);
-      free_workspace_keep_stream();
+        cudaMemcpy(ndI, dInst, (size_t)ninst_cap * sizeof(InstDev), cudaMemcpyDeviceToDevice);
+      free_workspace();
       hB = nb;
       hB.chunk_cap = cc;
       dB = ndB;
@@ -174,97 +251,161 @@ struct Engine {
       ninst_cap = nc;
       if (h_status) cudaFreeHost(h_status);
       if (cudaMallocHost(&h_status, (size_t)nc * sizeof(int2)) != cudaSuccess) return VFB_OOM;
-      if (step_exec) { cudaGraphExecDestroy(step_exec); step_exec = nullptr; }
+      if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
     }
     hB.inst = dInst;
     hB.ninst = ninst;
     if (cudaMemcpyAsync(dB, &hB, sizeof(BatchDev), cudaMemcpyHostToDevice, stream) != cudaSuccess)
       return VFB_DEVICE_ERROR;
+    c_h2d += sizeof(BatchDev);
     return VFB_OK;
   }
 
-  void free_workspace_keep_stream() {
-    auto f = [&](void* p) { if (p) cudaFreeAsync(p, stream); };
-    f(hB.p1_prefix); f(hB.chunk_prefix0); f(hB.chunk_prefix1); f(hB.tent_prefix); f(hB.win_prefix);
-    f(hB.chunk_cnt); f(hB.chunk_base); f(hB.tickets); f(hB.status_out); f(dB); f(dInst);
-  }
-
   // --------------------------------------------------------- step launch
-  void launch_step(int ninst, int p1_smem) {
+  void launch_step(int ninst, int p1_smem, bool timed) {
     const int g = grid;
+    int e = 0;
+    auto mark = [&]() { if (timed) cudaEventRecord(ev_k[e++], stream); };
+    mark();
     k_plan<<<1, 1024, 0, stream>>>(dB);
+    mark();
     k_p1<<<p1_grid, kTS, p1_smem, stream>>>(dB);
+    mark();
     for (int phase = 0; phase < 2; ++phase) {
-      if (phase == 1) k_verify<<<g, 256, 0, stream>>>(dB);
+      if (phase == 1) {
+        k_verify<<<g, 256, 0, stream>>>(dB);
+        mark();
+      }
       k_chunk_count<<<g, 256, 0, stream>>>(dB, phase);
+      mark();
       k_chunk_scan<<<std::min(ninst, g), kScanThreads, 0, stream>>>(dB, phase);
+      mark();
       k_chunk_emit<<<g, kChunkThreads, 0, stream>>>(dB, phase);
+      mark();
     }
     k_emit_rows<<<g, 256, 0, stream>>>(dB);
+    mark();
     k_finish<<<(ninst + 255) / 256, 256, 0, stream>>>(dB);
-    cudaMemcpyAsync(h_status, hB.status_out, (size_t)ninst * sizeof(int2), cudaMemcpyDeviceToHost, stream);
+    mark();
   }
 
-  cudaError_t run_step(int ninst, int p1_smem) {
-    if (!step_exec || step_ninst != ninst || step_smem != p1_smem || step_grid != p1_grid) {
-      if (step_exec) { cudaGraphExecDestroy(step_exec); step_exec = nullptr; }
-      cudaGraph_t graph;
-      cudaError_t e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
-      if (e != cudaSuccess) return e;
-      launch_step(ninst, p1_smem);
-      e = cudaStreamEndCapture(stream, &graph);
-      if (e != cudaSuccess) return e;
-      e = cudaGraphInstantiate(&step_exec, graph, 0);
-      cudaGraphDestroy(graph);
-      if (e != cudaSuccess) { step_exec = nullptr; return e; }
-      step_ninst = ninst;
-      step_smem = p1_smem;
-      step_grid = p1_grid;
+  // Graph: [loop: step + k_loop_ctl] + status read-back, or one step + status.
+  cudaError_t build_graph(int ninst, int p1_smem) {
+    if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaGraphCreate(&graph, 0);
+    if (e != cudaSuccess) return e;
+    bool loop = use_loop;
+    if (loop) {
+      cudaGraphConditionalHandle handle;
+      e = cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault);
+      cudaGraphNodeParams cp = {};
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = handle;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      cudaGraphNode_t cnode;
+      if (e == cudaSuccess) e = cudaGraphAddNode(&cnode, graph, nullptr, 0, &cp);
+      if (e == cudaSuccess) {
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        e = cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+          launch_step(ninst, p1_smem, false);
+          k_loop_ctl<<<1, 256, 0, stream>>>(dB, handle, kMaxLoop);
+          cudaGraph_t out = nullptr;
+          e = cudaStreamEndCapture(stream, &out);
+        }
+      }
+      if (e == cudaSuccess) {
+        // status read-back after the loop
+        e = cudaStreamBeginCaptureToGraph(stream, graph, &cnode, nullptr, 1, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+          cudaMemcpyAsync(h_status, hB.status_out, (size_t)ninst * sizeof(int2), cudaMemcpyDeviceToHost, stream);
+          cudaGraph_t out = nullptr;
+          e = cudaStreamEndCapture(stream, &out);
+        }
+      }
+      if (e != cudaSuccess) {
+        // no device-side loop on this driver: fall back to one step per launch
+        cudaGetLastError();
+        cudaGraphDestroy(graph);
+        graph = nullptr;
+        use_loop = false;
+        loop = false;
+        e = cudaGraphCreate(&graph, 0);
+        if (e != cudaSuccess) return e;
+      }
     }
-    return cudaGraphLaunch(step_exec, stream);
+    if (!loop) {
+      e = cudaStreamBeginCaptureToGraph(stream, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+      if (e != cudaSuccess) { cudaGraphDestroy(graph); return e; }
+      launch_step(ninst, p1_smem, profile != 0);
+      cudaMemcpyAsync(h_status, hB.status_out, (size_t)ninst * sizeof(int2), cudaMemcpyDeviceToHost, stream);
+      cudaGraph_t out = nullptr;
+      e = cudaStreamEndCapture(stream, &out);
+      if (e != cudaSuccess) { cudaGraphDestroy(graph); return e; }
+    }
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) { exec = nullptr; return e; }
+    exec_ninst = ninst;
+    exec_smem = p1_smem;
+    exec_grid = p1_grid;
+    exec_loop = loop;
+    return cudaSuccess;
+  }
+
+  cudaError_t run(int ninst, int p1_smem) {
+    if (!exec || exec_ninst != ninst || exec_smem != p1_smem || exec_grid != p1_grid ||
+        exec_loop != (int)use_loop) {
+      const cudaError_t e = build_graph(ninst, p1_smem);
+      if (e != cudaSuccess) return e;
+    }
+    if (exec_loop) cudaMemsetAsync(hB.loop_iter, 0, sizeof(unsigned long long), stream);
+    c_d2h += (uint64_t)ninst * sizeof(int2);
+    return cudaGraphLaunch(exec, stream);
   }
 
   // ------------------------------------------------------ instance buffers
   vfb_status alloc_buffers(InstHost& H, uint64_t rows, uint64_t slots, uint64_t words, uint64_t tents) {
     InstDev& d = H.d;
-    void* p;
-    const size_t rb = rows * (size_t)d.TP * 8, ob = rows * 8, tb = slots * sizeof(Slot), bb = words * 4,
-                 eb = tents * 8;
-    if (dalloc(&p, rb) != cudaSuccess) return VFB_OOM;
-    d.rows = (uint64_t*)p;
-    if (dalloc(&p, ob) != cudaSuccess) return VFB_OOM;
-    d.origin = (uint64_t*)p;
-    if (dalloc(&p, tb) != cudaSuccess) return VFB_OOM;
-    d.table = (Slot*)p;
-    if (dalloc(&p, bb) != cudaSuccess) return VFB_OOM;
-    d.bitmap = (uint32_t*)p;
-    if (dalloc(&p, eb) != cudaSuccess) return VFB_OOM;
-    d.tent = (uint64_t*)p;
-    if (dalloc(&p, eb) != cudaSuccess) return VFB_OOM;
-    d.wins = (uint64_t*)p;
-    cudaMemsetAsync(d.table, 0xFF, tb, stream);
-    cudaMemsetAsync(d.bitmap, 0, bb, stream);
-    cudaMemsetAsync(d.rows, 0, rb, stream);
-    d.row_cap = rows;
-    d.table_mask = slots - 1;
-    d.bitmap_words = words;
-    d.tent_cap = tents;
-    H.bytes = rb + ob + tb + bb + 2 * eb;
+    size_t g1, g2, g3, g4, g5, g6;
+    void* pr = dalloc(rows * (size_t)d.TP * 8, &g1);
+    void* po = dalloc(rows * 8, &g2);
+    void* pt = dalloc(slots * sizeof(Slot), &g3);
+    void* pb = dalloc(words * 4, &g4);
+    void* pe = dalloc(tents * 8, &g5);
+    void* pw = dalloc(tents * 8, &g6);
+    if (!pr || !po || !pt || !pb || !pe || !pw) {
+      dfree(pr); dfree(po); dfree(pt); dfree(pb); dfree(pe); dfree(pw);
+      return VFB_OOM;
+    }
+    d.rows = (uint64_t*)pr;
+    d.origin = (uint64_t*)po;
+    d.row_cap = std::min<uint64_t>(g1 / ((size_t)d.TP * 8), g2 / 8);
+    d.table = (Slot*)pt;
+    d.table_mask = pow2_at_most(g3 / sizeof(Slot)) - 1;
+    d.bitmap = (uint32_t*)pb;
+    d.bitmap_words = g4 / 4;
+    d.tent = (uint64_t*)pe;
+    d.wins = (uint64_t*)pw;
+    d.tent_cap = std::min(g5, g6) / 8;
+    cudaMemsetAsync(d.table, 0xFF, (d.table_mask + 1) * sizeof(Slot), stream);
+    cudaMemsetAsync(d.bitmap, 0, d.bitmap_words * 4, stream);
     return VFB_OK;
   }
 
   void free_buffers(InstHost& H) {
     InstDev& d = H.d;
-    dfree(d.rows, d.row_cap * (size_t)d.TP * 8);
-    dfree(d.origin, d.row_cap * 8);
-    dfree(d.table, (d.table_mask + 1) * sizeof(Slot));
-    dfree(d.bitmap, d.bitmap_words * 4);
-    dfree(d.tent, d.tent_cap * 8);
-    dfree(d.wins, d.tent_cap * 8);
+    dfree(d.rows);
+    dfree(d.origin);
+    dfree(d.table);
+    dfree(d.bitmap);
+    dfree(d.tent);
+    dfree(d.wins);
     d.rows = d.origin = d.tent = d.wins = nullptr;
     d.table = nullptr;
     d.bitmap = nullptr;
-    H.bytes = 0;
   }
 
   // Grow whatever the device asked for; the level is then re-run.
@@ -272,68 +413,69 @@ struct Engine {
     InstDev& d = H.d;
     if (cudaMemcpyAsync(&d, dInst + idx, sizeof(InstDev), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
       return VFB_DEVICE_ERROR;
+    c_d2h += sizeof(InstDev);
     if (cudaStreamSynchronize(stream) != cudaSuccess) return VFB_DEVICE_ERROR;
     const int need = d.need;
-    void* p;
+    size_t g1, g2;
     if (need & NEED_LIMIT) return VFB_LIMIT;
     if (need & NEED_ROWS) {
       const uint64_t want = std::max<uint64_t>(2 * d.row_cap, d.need_amount[3] + d.need_amount[3] / 4);
       const uint64_t used = d.lstart[d.level];
-      if (dalloc(&p, want * (size_t)d.TP * 8) != cudaSuccess) return VFB_OOM;
-      uint64_t* nr = (uint64_t*)p;
-      cudaMemcpyAsync(nr, d.rows, used * (size_t)d.TP * 8, cudaMemcpyDeviceToDevice, stream);
-      if (dalloc(&p, want * 8) != cudaSuccess) { dfree(nr, want * (size_t)d.TP * 8); return VFB_OOM; }
-      uint64_t* no = (uint64_t*)p;
-      cudaMemcpyAsync(no, d.origin, used * 8, cudaMemcpyDeviceToDevice, stream);
-      dfree(d.rows, d.row_cap * (size_t)d.TP * 8);
-      dfree(d.origin, d.row_cap * 8);
-      H.bytes += (want - d.row_cap) * ((size_t)d.TP * 8 + 8);
-      d.rows = nr;
-      d.origin = no;
-      d.row_cap = want;
+      void* pr = dalloc(want * (size_t)d.TP * 8, &g1);
+      void* po = pr ? dalloc(want * 8, &g2) : nullptr;
+      if (!pr || !po) { dfree(pr); return VFB_OOM; }
+      cudaMemcpyAsync(pr, d.rows, used * (size_t)d.TP * 8, cudaMemcpyDeviceToDevice, stream);
+      cudaMemcpyAsync(po, d.origin, used * 8, cudaMemcpyDeviceToDevice, stream);
+      dfree(d.rows);
+      dfree(d.origin);
+      d.rows = (uint64_t*)pr;
+      d.origin = (uint64_t*)po;
+      d.row_cap = std::min<uint64_t>(g1 / ((size_t)d.TP * 8), g2 / 8);
     }
     if (need & NEED_TABLE) {
       const uint64_t cap = d.table_mask + 1;
       const uint64_t want = pow2_at_least(std::max<uint64_t>(2 * cap, d.need_amount[1]));
-      if (dalloc(&p, want * sizeof(Slot)) != cudaSuccess) return VFB_OOM;
-      Slot* nt = (Slot*)p;
-      cudaMemsetAsync(nt, 0xFF, want * sizeof(Slot), stream);
+      void* pt = dalloc(want * sizeof(Slot), &g1);
+      if (!pt) return VFB_OOM;
+      const uint64_t slots = pow2_at_most(g1 / sizeof(Slot));
+      cudaMemsetAsync(pt, 0xFF, slots * sizeof(Slot), stream);
       cudaMemsetAsync(d_fail, 0, sizeof(unsigned long long), stream);
-      k_rehash<<<grid, 256, 0, stream>>>(d.table, cap, nt, want - 1, d_fail);
+      k_rehash<<<grid, 256, 0, stream>>>(d.table, cap, (Slot*)pt, slots - 1, d_fail);
+      ++c_launch;
       unsigned long long fails = 0;
       cudaMemcpyAsync(&fails, d_fail, sizeof(fails), cudaMemcpyDeviceToHost, stream);
+      c_d2h += sizeof(fails);
       if (cudaStreamSynchronize(stream) != cudaSuccess) return VFB_DEVICE_ERROR;
       if (fails) return VFB_DEVICE_ERROR;
-      dfree(d.table, cap * sizeof(Slot));
-      H.bytes += (want - cap) * sizeof(Slot);
-      d.table = nt;
-      d.table_mask = want - 1;
+      dfree(d.table);
+      d.table = (Slot*)pt;
+      d.table_mask = slots - 1;
     }
     if (need & NEED_BITMAP) {
       const uint64_t want = std::max<uint64_t>(2 * d.bitmap_words, d.need_amount[0] + d.need_amount[0] / 4);
-      if (dalloc(&p, want * 4) != cudaSuccess) return VFB_OOM;
-      cudaMemsetAsync(p, 0, want * 4, stream);
-      dfree(d.bitmap, d.bitmap_words * 4);
-      H.bytes += (want - d.bitmap_words) * 4;
-      d.bitmap = (uint32_t*)p;
-      d.bitmap_words = want;
+      void* pb = dalloc(want * 4, &g1);
+      if (!pb) return VFB_OOM;
+      cudaMemsetAsync(pb, 0, g1 / 4 * 4, stream);
+      dfree(d.bitmap);
+      d.bitmap = (uint32_t*)pb;
+      d.bitmap_words = g1 / 4;
     }
     if (need & NEED_TENT) {
       const uint64_t want = std::max<uint64_t>(2 * d.tent_cap, d.need_amount[2] + d.need_amount[2] / 4);
-      void* q;
-      if (dalloc(&p, want * 8) != cudaSuccess) return VFB_OOM;
-      if (dalloc(&q, want * 8) != cudaSuccess) { dfree(p, want * 8); return VFB_OOM; }
-      dfree(d.tent, d.tent_cap * 8);
-      dfree(d.wins, d.tent_cap * 8);
-      H.bytes += (want - d.tent_cap) * 16;
-      d.tent = (uint64_t*)p;
-      d.wins = (uint64_t*)q;
-      d.tent_cap = want;
+      void* pe = dalloc(want * 8, &g1);
+      void* pw = pe ? dalloc(want * 8, &g2) : nullptr;
+      if (!pe || !pw) { dfree(pe); return VFB_OOM; }
+      dfree(d.tent);
+      dfree(d.wins);
+      d.tent = (uint64_t*)pe;
+      d.wins = (uint64_t*)pw;
+      d.tent_cap = std::min(g1, g2) / 8;
     }
     d.status = ST_RUNNING;
     d.need = 0;
     if (cudaMemcpyAsync(dInst + idx, &d, sizeof(InstDev), cudaMemcpyHostToDevice, stream) != cudaSuccess)
       return VFB_DEVICE_ERROR;
+    c_h2d += sizeof(InstDev);
     return VFB_OK;
   }
 
@@ -396,22 +538,80 @@ struct Engine {
     return VFB_OK;
   }
 
-  vfb_status upload_atoms(const vfb_instance& in, InstHost& H, std::vector<uint64_t>& staging) {
-    const InstDev& d = H.d;
-    staging.assign((size_t)d.A * d.TP, 0ULL);
-    for (int v = 0; v < d.A; ++v)
-      for (int t = 0; t < d.T; ++t) staging[(size_t)v * d.TP + t] = in.words[(size_t)t * d.A + v];
-    if (cudaMemcpyAsync(d.rows, staging.data(), staging.size() * 8, cudaMemcpyHostToDevice, stream) !=
-        cudaSuccess)
-      return VFB_DEVICE_ERROR;
-    // the copy reads pageable memory: it completes before the call returns
+  vfb_status upload_atoms(const vfb_instance* ins, std::vector<InstHost>& H, int n) {
+    size_t words = 0;
+    for (int i = 0; i < n; ++i)
+      if (H[i].active) words += (size_t)H[i].d.A * H[i].d.TP;
+    if (words > h_stage_words) {
+      if (h_stage) cudaFreeHost(h_stage);
+      h_stage = nullptr;
+      h_stage_words = 0;
+      if (cudaMallocHost(&h_stage, words * 8) != cudaSuccess) return VFB_OOM;
+      h_stage_words = words;
+    }
+    size_t o = 0;
+    for (int i = 0; i < n; ++i) {
+      if (!H[i].active) continue;
+      const InstDev& d = H[i].d;
+      uint64_t* dst = h_stage + o;
+      for (int v = 0; v < d.A; ++v) {
+        for (int t = 0; t < d.T; ++t) dst[(size_t)v * d.TP + t] = ins[i].words[(size_t)t * d.A + v];
+        if (d.TP > d.T) dst[(size_t)v * d.TP + d.T] = 0;
+      }
+      const size_t nb = (size_t)d.A * d.TP * 8;
+      if (cudaMemcpyAsync(d.rows, dst, nb, cudaMemcpyHostToDevice, stream) != cudaSuccess)
+        return VFB_DEVICE_ERROR;
+      c_h2d += nb;
+      o += (size_t)d.A * d.TP;
+    }
     return VFB_OK;
+  }
+
+  // bytes each kernel of one level step had to move (see vfb_kernel_stat)
+  void account_level(const InstDev& d, int k) {
+    const double T8 = 8.0 * d.T;
+    const uint64_t* n = d.lcount;
+    double operands = (double)n[k - 1] * T8;
+    for (int i = 1; 2 * i <= k - 1; ++i) {
+      const int j = k - 1 - i;
+      operands += (double)(i == j ? n[i] : n[i] + n[j]) * T8;
+    }
+    const double cands = (double)d.cands, tent = (double)d.n_tent, wins = (double)d.n_wins;
+    const double w0 = std::ceil(cands / 32.0) * 4, w1 = std::ceil(tent / 32.0) * 4;
+    prof[KP_P1].bytes += operands + 32.0 * cands + 4.0 * tent;
+    prof[KP_COUNT].bytes += w0 + w1;
+    prof[KP_EMIT].bytes += w0 + w1 + 8.0 * tent + 16.0 * wins;
+    prof[KP_VERIFY].bytes += tent * (2 * T8 + 32 + 8 + 4);
+    prof[KP_ROWS].bytes += wins * (2 * T8 + 8.0 * d.TP + 16);
+  }
+
+  void profile_step(int n, std::vector<InstHost>& H) {
+    float ms[kStepLen];
+    for (int j = 0; j < kStepLen; ++j) {
+      ms[j] = 0;
+      cudaEventElapsedTime(&ms[j], ev_k[j], ev_k[j + 1]);
+      prof[kStepSeq[j]].launches += 1;
+      prof[kStepSeq[j]].ms += ms[j];
+    }
+    std::vector<InstDev> recs(n);
+    cudaMemcpy(recs.data(), dInst, (size_t)n * sizeof(InstDev), cudaMemcpyDeviceToHost);
+    for (int i = 0; i < n; ++i) {
+      const InstDev& d = recs[i];
+      const int k = d.res_size;
+      if (H[i].active && k > H[i].accounted && k >= 2 && k <= kMaxSize &&
+          (d.status == ST_FOUND || d.status == ST_NOT_FOUND || d.level == k + 1)) {
+        account_level(d, k);
+        H[i].accounted = k;
+      }
+    }
   }
 
   vfb_status batch(const vfb_instance* ins, int n, vfb_result* out) {
     const auto t0 = std::chrono::steady_clock::now();
     if (n <= 0) return VFB_OK;
     if (cudaSetDevice(device) != cudaSuccess) return VFB_DEVICE_ERROR;
+    c_h2d = c_d2h = c_launch = 0;
+    cudaEventRecord(ev_t0, stream);
     std::vector<InstHost> H(n);
     int maxTP = 2;
     for (int i = 0; i < n; ++i) {
@@ -430,19 +630,17 @@ struct Engine {
     p1_grid = sms * std::max(occ, 1);
 
     vfb_status rc = VFB_OK;
-    std::vector<uint64_t> staging;
     uint64_t chunk_need = 0;
-    for (int i = 0; i < n && rc == VFB_OK; ++i) {
+    for (int i = 0; i < n; ++i) {
       if (H[i].fail != VFB_OK) continue;
       const InstDev& d = H[i].d;
       const uint64_t rows = std::max<uint64_t>(4096, (uint64_t)d.A * 16);
       const vfb_status s = alloc_buffers(H[i], rows, 1 << 14, 1 << 14, 1 << 13);
       if (s != VFB_OK) { H[i].fail = s; H[i].d.status = ST_IDLE; continue; }
-      const vfb_status u = upload_atoms(ins[i], H[i], staging);
-      if (u != VFB_OK) { rc = u; break; }
       H[i].active = true;
       chunk_need += (H[i].d.bitmap_words + kChunkWords - 1) / kChunkWords;
     }
+    rc = upload_atoms(ins, H, n);
     if (rc == VFB_OK) rc = ensure_workspace(n, chunk_need + n);
     if (rc == VFB_OK) {
       std::vector<InstDev> recs(n);
@@ -450,66 +648,95 @@ struct Engine {
       if (cudaMemcpyAsync(dInst, recs.data(), (size_t)n * sizeof(InstDev), cudaMemcpyHostToDevice, stream) !=
           cudaSuccess)
         rc = VFB_DEVICE_ERROR;
-      if (cudaStreamSynchronize(stream) != cudaSuccess) rc = VFB_DEVICE_ERROR;
+      c_h2d += (uint64_t)n * sizeof(InstDev);
+      // pageable source: the copy has been staged when the call returns
     }
     if (rc == VFB_OK) {
+      if (profile) cudaEventRecord(ev_k[0], stream);
       k_init<<<std::min(n, grid), 256, 0, stream>>>(dB);
-      if (cudaMemcpyAsync(h_status, hB.status_out, (size_t)n * sizeof(int2), cudaMemcpyDeviceToHost, stream) !=
-              cudaSuccess ||
-          cudaStreamSynchronize(stream) != cudaSuccess)
-        rc = VFB_DEVICE_ERROR;
+      ++c_launch;
+      if (profile) {
+        cudaEventRecord(ev_k[1], stream);
+        cudaStreamSynchronize(stream);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ev_k[0], ev_k[1]);
+        prof[KP_INIT].launches += 1;
+        prof[KP_INIT].ms += ms;
+      }
     }
     int guard = 0;
+    bool first = true;
     while (rc == VFB_OK) {
-      bool running = false;
-      for (int i = 0; i < n; ++i) {
-        if (!H[i].active) continue;
-        const int st = h_status[i].x;
-        if (st == ST_RUNNING) running = true;
-        if (st == ST_NEED_MEM) {
-          const vfb_status g = grow(H[i], i);
-          if (g != VFB_OK) {
-            // this instance stops; the others carry on
-            H[i].fail = g;
-            H[i].active = false;
-            InstDev& d = H[i].d;
-            d.status = ST_ERROR;
-            cudaMemcpyAsync(&dInst[i].status, &d.status, sizeof(int), cudaMemcpyHostToDevice, stream);
-            if (g == VFB_DEVICE_ERROR) rc = g;
-          } else {
-            running = true;
+      if (!first) {
+        bool running = false, grew = false;
+        for (int i = 0; i < n; ++i) {
+          if (!H[i].active) continue;
+          const int st = h_status[i].x;
+          if (st == ST_RUNNING) running = true;
+          if (st == ST_NEED_MEM) {
+            const vfb_status g = grow(H[i], i);
+            if (g != VFB_OK) {
+              // this instance stops; the others carry on
+              H[i].fail = g;
+              H[i].active = false;
+              const int err = ST_ERROR;
+              cudaMemcpyAsync(&dInst[i].status, &err, sizeof(int), cudaMemcpyHostToDevice, stream);
+              cudaStreamSynchronize(stream);
+              c_h2d += sizeof(int);
+              if (g == VFB_DEVICE_ERROR) rc = g;
+            } else {
+              running = grew = true;
+            }
+          }
+          if (st == ST_ERROR) { H[i].fail = VFB_DEVICE_ERROR; H[i].active = false; }
+        }
+        if (!running || rc != VFB_OK) break;
+        if (grew) {
+          uint64_t cn = 0;
+          for (int i = 0; i < n; ++i)
+            if (H[i].d.bitmap) cn += (H[i].d.bitmap_words + kChunkWords - 1) / kChunkWords;
+          if (cn + n > hB.chunk_cap) {
+            rc = ensure_workspace(n, cn + n);
+            if (rc != VFB_OK) break;
           }
         }
-        if (st == ST_ERROR) { H[i].fail = VFB_DEVICE_ERROR; H[i].active = false; }
       }
-      if (!running || rc != VFB_OK) break;
-      // the bitmap compaction needs room for every instance's chunks
-      uint64_t cn = 0;
-      for (int i = 0; i < n; ++i)
-        if (H[i].d.bitmap) cn += (H[i].d.bitmap_words + kChunkWords - 1) / kChunkWords;
-      if (cn + n > hB.chunk_cap) {
-        rc = ensure_workspace(n, cn + n);
-        if (rc != VFB_OK) break;
-      }
-      cudaError_t e = run_step(n, p1_smem);
+      first = false;
+      cudaError_t e = run(n, p1_smem);
       if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
       if (e != cudaSuccess) { last_error = e; rc = VFB_DEVICE_ERROR; break; }
+      c_launch += exec_loop ? 0 : (uint64_t)kStepLen;
+      if (exec_loop) {
+        unsigned long long it = 0;
+        cudaMemcpy(&it, hB.loop_iter, sizeof(it), cudaMemcpyDeviceToHost);
+        c_d2h += sizeof(it);
+        c_launch += it * (kStepLen + 1);
+      }
+      if (profile) profile_step(n, H);
       if (verbose) report_progress(n);
       if (++guard > 64 * kMaxSize) { rc = VFB_DEVICE_ERROR; break; }
     }
     // results
     std::vector<InstDev> recs(n);
     if (cudaMemcpyAsync(recs.data(), dInst, (size_t)n * sizeof(InstDev), cudaMemcpyDeviceToHost, stream) !=
-            cudaSuccess ||
-        cudaStreamSynchronize(stream) != cudaSuccess) {
+            cudaSuccess) {
       if (rc == VFB_OK) rc = VFB_DEVICE_ERROR;
     }
+    c_d2h += (uint64_t)n * sizeof(InstDev);
+    cudaEventRecord(ev_t1, stream);
+    if (cudaStreamSynchronize(stream) != cudaSuccess && rc == VFB_OK) rc = VFB_DEVICE_ERROR;
+    float dev_ms = 0;
+    cudaEventElapsedTime(&dev_ms, ev_t0, ev_t1);
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     for (int i = 0; i < n; ++i) {
       vfb_result& r = out[i];
       const InstDev& d = recs[i];
       r.seconds = secs;
-      if (H[i].fail != VFB_OK && !(H[i].d.rows)) {
+      r.device_seconds = dev_ms * 1e-3;
+      r.h2d_bytes = c_h2d;
+      r.d2h_bytes = c_d2h;
+      r.kernel_launches = c_launch;
+      if (H[i].fail != VFB_OK && !H[i].d.rows) {
         r.status = H[i].fail;
         continue;
       }
@@ -532,8 +759,8 @@ struct Engine {
         r.status = VFB_NOT_FOUND;
       } else {
         r.status = H[i].fail != VFB_OK ? H[i].fail : (rc != VFB_OK ? rc : VFB_DEVICE_ERROR);
-        // level counts of the last level are not final
-        if (r.size >= 1 && d.status != ST_FOUND) {
+        // the level in progress is not complete: report the finished ones
+        if (r.size >= 1 && d.level <= r.size) {
           r.total_rows -= r.level_rows[r.size];
           r.level_rows[r.size] = 0;
           r.level_cands[r.size] = 0;
@@ -543,7 +770,6 @@ struct Engine {
     }
     for (int i = 0; i < n; ++i)
       if (H[i].d.rows) free_buffers(H[i]);
-    cudaStreamSynchronize(stream);
     return rc;
   }
 
@@ -554,9 +780,24 @@ struct Engine {
       if (d.status == ST_NEED_MEM) continue;
       const int k = d.res_size;
       if (k < 1 || k > kMaxSize) continue;
-      std::fprintf(stderr, "Length %-2d | (all) | CheckedLTLs: %-13llu | UniqueCS: %-12llu\n", k,
-                   (unsigned long long)d.lcands[k], (unsigned long long)d.lcount[k]);
+      for (int j = 2; j <= k; ++j)
+        std::fprintf(stderr, "Length %-2d | (all) | CheckedLTLs: %-13llu | UniqueCS: %-12llu\n", j,
+                     (unsigned long long)d.lcands[j], (unsigned long long)d.lcount[j]);
     }
+  }
+
+  int profile_read(vfb_kernel_stat* outp, int cap) {
+    int m = 0;
+    for (int k = 0; k < KP_N && m < cap; ++k) {
+      if (!prof[k].launches) continue;
+      vfb_kernel_stat& s = outp[m++];
+      std::memset(&s, 0, sizeof(s));
+      std::snprintf(s.name, sizeof(s.name), "%s", kNames[k]);
+      s.launches = prof[k].launches;
+      s.ms = prof[k].ms;
+      s.bytes = prof[k].bytes;
+    }
+    return m;
   }
 };
 
@@ -605,6 +846,17 @@ vfb_status vfb_solve(void* ctx, const vfb_instance* inst, vfb_result* out) {
 vfb_status vfb_batch_solve(void* ctx, const vfb_instance* inst, int n, vfb_result* out) {
   if (!ctx || (n > 0 && (!inst || !out)) || n < 0) return VFB_BAD_INPUT;
   return static_cast<Engine*>(ctx)->batch(inst, n, out);
+}
+
+int vfb_profile_read(void* ctx, vfb_kernel_stat* out, int cap) {
+  if (!ctx || !out || cap <= 0) return 0;
+  return static_cast<Engine*>(ctx)->profile_read(out, cap);
+}
+
+void vfb_profile_reset(void* ctx) {
+  if (!ctx) return;
+  Engine* e = static_cast<Engine*>(ctx);
+  for (auto& p : e->prof) p = vfb::Prof{};
 }
 
 }  // extern "C"

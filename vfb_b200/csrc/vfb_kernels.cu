@@ -796,6 +796,27 @@ __global__ void k_finish(BatchDev* Bp) {
   }
 }
 
+__global__ void k_loop_ctl(BatchDev* Bp, cudaGraphConditionalHandle handle, unsigned int max_iter) {
+  __shared__ int s_run, s_need;
+  const BatchDev B = *Bp;
+  if (threadIdx.x == 0) { s_run = 0; s_need = 0; }
+  __syncthreads();
+  int run = 0, need = 0;
+  for (int b = threadIdx.x; b < B.ninst; b += blockDim.x) {
+    const int st = B.status_out[b].x;
+    run |= (st == ST_RUNNING);
+    need |= (st == ST_NEED_MEM);
+  }
+  if (run) atomicOr(&s_run, 1);
+  if (need) atomicOr(&s_need, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned long long it = ++(*B.loop_iter);
+    const bool more = s_run && !s_need && it < max_iter;
+    cudaGraphSetConditional(handle, more ? 1u : 0u);
+  }
+}
+
 // ==================================================================== init
 // Level 1: every proposition is a row (duplicates included); its key enters
 // the set; propositions are tested as size-1 solutions in order

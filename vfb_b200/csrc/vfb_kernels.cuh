@@ -24,6 +24,7 @@ struct BatchDev {
   unsigned long long chunk_cap;
   unsigned long long* tickets;          // [4]: P1 work ticket, scan0/scan1 done counters
   int2* status_out;                     // [ninst] (status, need) mirror for the host
+  unsigned long long* loop_iter;        // level steps run by the current device-side loop
 };
 
 // Level-step kernels, launched in this order for every level.
@@ -35,6 +36,9 @@ __global__ void k_chunk_emit(BatchDev* B, int phase);
 __global__ void k_verify(BatchDev* B);
 __global__ void k_emit_rows(BatchDev* B);
 __global__ void k_finish(BatchDev* B);
+// Device-side level loop: keeps the graph's while-node running while some
+// instance is RUNNING, none waits for memory and fewer than max_iter steps ran.
+__global__ void k_loop_ctl(BatchDev* B, cudaGraphConditionalHandle handle, unsigned int max_iter);
 
 // Set-up and maintenance kernels.
 __global__ void k_init(BatchDev* B);
