@@ -41,7 +41,8 @@ class _Problem(ctypes.Structure):
                 ("threads", ctypes.c_int), ("ref_max_pitch", ctypes.c_int64),
                 ("max_rows", ctypes.c_uint64),
                 ("len", ctypes.POINTER(ctypes.c_uint8)),
-                ("atoms", ctypes.POINTER(ctypes.c_uint64))]
+                ("atoms", ctypes.POINTER(ctypes.c_uint64)),
+                ("trace", ctypes.POINTER(ctypes.c_int64)), ("trace_cap", ctypes.c_int)]
 
 
 class _Result(ctypes.Structure):
@@ -50,7 +51,8 @@ class _Result(ctypes.Structure):
                 ("level_rows", ctypes.c_uint64 * (MAX_SIZE + 1)),
                 ("level_cands", ctypes.c_uint64 * (MAX_SIZE + 1)),
                 ("solution_index", ctypes.c_uint64),
-                ("total_rows", ctypes.c_uint64), ("seconds", ctypes.c_double)]
+                ("total_rows", ctypes.c_uint64), ("seconds", ctypes.c_double),
+                ("trace_len", ctypes.c_int)]
 
 
 _lib = None
@@ -89,10 +91,12 @@ class Problem:
         self._len = (ctypes.c_uint8 * t)(*lengths)
         flat = [w for row in atoms for w in row]
         self._atoms = (ctypes.c_uint64 * max(1, len(flat)))(*flat)
+        self._trace = (ctypes.c_int64 * (5 * 4096))()
         self.p = _Problem(t, num_pos, a, max_size, rlx_type, mode, threads,
                           ref_max_pitch, max_rows,
                           ctypes.cast(self._len, ctypes.POINTER(ctypes.c_uint8)),
-                          ctypes.cast(self._atoms, ctypes.POINTER(ctypes.c_uint64)))
+                          ctypes.cast(self._atoms, ctypes.POINTER(ctypes.c_uint64)),
+                          ctypes.cast(self._trace, ctypes.POINTER(ctypes.c_int64)), 4096)
 
     @classmethod
     def from_instance(cls, inst, **kw):
@@ -126,7 +130,12 @@ def _result(r: _Result) -> dict:
 def solve(prob: Problem) -> dict:
     r = _Result()
     lib().orc_solve(ctypes.byref(prob.p), ctypes.byref(r))
-    return _result(r)
+    out = _result(r)
+    tr = prob._trace
+    # LTL_BS progress lines: (cost, op, AllLTLs, StoredLTLs, ToBeChecked)
+    out["launches"] = [(int(tr[5 * i]), "~&|XFGUA"[tr[5 * i + 1]], int(tr[5 * i + 2]),
+                        int(tr[5 * i + 3]), int(tr[5 * i + 4])) for i in range(r.trace_len)]
+    return out
 
 
 def exhaustive(prob: Problem, max_formulas: int = 1 << 26) -> dict:

@@ -267,7 +267,24 @@ typedef struct {
     uint64_t found_g;
     int error;             /* ORC_LIMIT on row budget / allocation failure */
     uint64_t *tmp;
+    uint64_t all_ltls;     /* LTL_BS's AllLTLs counter (ref-compat trace) */
+    int trace_len;
 } search_t;
+
+/* One LTL_BS progress line, printed before each launch. */
+static void trace_launch(search_t *s, int cost, int op, uint64_t n_printed) {
+    const orc_problem *p = s->p;
+    if (p->trace && s->trace_len < p->trace_cap) {
+        int64_t *e = p->trace + 5 * (size_t)s->trace_len;
+        e[0] = cost;
+        e[1] = op;
+        e[2] = (int64_t)s->all_ltls;
+        e[3] = (int64_t)s->rows.n;
+        e[4] = (int64_t)n_printed;
+        s->trace_len++;
+    }
+    s->all_ltls += n_printed;
+}
 
 static inline const uint64_t *row_cs(const search_t *s, int64_t r) {
     return s->rows.cs + (size_t)r * s->T;
@@ -343,6 +360,7 @@ static int level_refcompat(search_t *s, int k) {
             int64_t x = u0, y;
             do {
                 y = x + ((temp - 1) < (u1 - x) ? (temp - 1) : (u1 - x));
+                trace_launch(s, k, op, (uint64_t)(y - x + 1));
                 for (int64_t a = x; a <= y; ++a)
                     if (process(s, op, a, -1)) return 1;
                 x = y + 1;
@@ -361,6 +379,7 @@ static int level_refcompat(search_t *s, int k) {
                 y = x + (cw < (i4 - x) ? cw : (i4 - x));
                 const int64_t w = y - x + 1;
                 const int64_t n = w * nl;
+                trace_launch(s, k, op, (uint64_t)(op == OP_U ? 2 * n : n));
                 if (op != OP_U) {
                     for (int64_t t = 0; t < n; ++t)
                         if (process(s, op, i1 + t / w, x + t % w)) return 1;
@@ -538,7 +557,10 @@ int orc_solve(const orc_problem *p, orc_result *res) {
      * proposition order (LTL_BS.cu:1127-1163, 1217). */
     s.level = 1;
     s.lvl_start[1] = 0;
+    trace_launch(&s, 1, 7, (uint64_t)p->num_vars);
+    s.all_ltls = 0;
     for (int v = 0; v < p->num_vars; ++v) {
+        s.all_ltls++;
         uint64_t *cs = s.rows.cs + (size_t)v * s.T;
         for (int i = 0; i < s.T; ++i) cs[i] = p->atoms[(size_t)v * s.T + i];
         s.rows.op[v] = OP_NONE;
@@ -587,6 +609,7 @@ int orc_solve(const orc_problem *p, orc_result *res) {
         res->status = ORC_NOT_FOUND;
     }
     res->total_rows = s.rows.n;
+    res->trace_len = s.trace_len;
 done:
     kset_free(&s.set);
     rows_free(&s.rows);

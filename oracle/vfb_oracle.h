@@ -49,6 +49,10 @@ typedef struct {
     uint64_t max_rows;         /* row budget; exceeding it returns ORC_LIMIT */
     const uint8_t *len;        /* [num_traces], 1..64 */
     const uint64_t *atoms;     /* [num_vars][num_traces] proposition words */
+    int64_t *trace;            /* ref-compat launch log, 5 words per launch: cost, op
+                                  (0..6, 7 = atoms), AllLTLs, StoredLTLs, ToBeChecked as
+                                  printed before each launch (LTL_BS.cu:1193, 1230, ...) */
+    int trace_cap;             /* launches the trace buffer can hold */
 } orc_problem;
 
 typedef struct {
@@ -61,6 +65,7 @@ typedef struct {
     uint64_t solution_index;   /* canonical candidate index of the solution within its level */
     uint64_t total_rows;
     double seconds;
+    int trace_len;             /* launches written to problem->trace */
 } orc_result;
 
 /* Solve one instance.  Returns result->status. */

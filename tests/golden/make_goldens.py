@@ -1,0 +1,83 @@
+"""Generates tests/golden/reference_runs.json by running the reference's own
+programs (built from its sources into oracle/_ref by oracle.reference) on a
+GPU machine:
+
+  ltl_nocache <json> <max_size>                         -> formula (stdout)
+  ltl_bs <txt> 1 1 1 1 1 1 1 1 <max> <max> <rlx> 1      -> progress lines + formula
+
+over a fixed list of seeded instances (small exact-key ones, relaxed-key ones
+run with each relaxed-uniqueness rule, and the two smallest benchmark shapes).
+The fixture stores each instance's trace JSON inline with the raw outputs, so
+the CPU tests need neither a GPU nor the reference sources.
+
+Usage (on a machine with a B200):  python tests/golden/make_goldens.py
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+import tempfile
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from oracle import reference  # noqa: E402
+from vfb_b200 import synth  # noqa: E402
+
+OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_runs.json")
+
+
+def instances():
+    out = []
+    out.append((synth.config_small(), 10, [3]))
+    out.append((synth.config_planted(), 13, [1, 2, 3]))
+    # exact keys (total trace bits <= 126)
+    for s in range(10):
+        rng = synth.Rng(7000 + s)
+        a = 2 + rng.below(2)
+        t = 3 + rng.below(5)
+        size = 3 + rng.below(4)
+        inst = synth.planted_instance(rng, a, size, t // 2 + 1, t - t // 2,
+                                      lambda: 3 + rng.below(8), 0.5, size + 1, name=f"exact{s}")
+        if sum(inst.lengths()) <= 126:
+            out.append((inst, size + 1, [3]))
+    # relaxed keys (more than 126 trace bits): every rule
+    for s in range(8):
+        rng = synth.Rng(8000 + s)
+        a = 2 + rng.below(3)
+        t = 10 + rng.below(20)
+        size = 4 + rng.below(4)
+        inst = synth.planted_instance(rng, a, size, t // 2, t - t // 2,
+                                      lambda: 8 + rng.below(24), 0.5, size + 1, name=f"relaxed{s}")
+        out.append((inst, size + 1, [1, 2, 3]))
+    return out
+
+
+def main():
+    if not reference.build_if_present():
+        if not reference.available():
+            raise SystemExit("reference programs are not built (oracle/_ref)")
+    runs = []
+    with tempfile.TemporaryDirectory() as tmp:
+        for idx, (inst, max_size, rlx_types) in enumerate(instances()):
+            name = inst.name or f"inst{idx}"
+            jpath = os.path.join(tmp, f"{name}.json")
+            tpath = os.path.join(tmp, f"{name}.txt")
+            inst.write_json(jpath)
+            with open(tpath, "w") as f:
+                f.write(reference.instance_to_text(inst))
+            rec = {"name": name, "max_size": max_size, "json": inst.to_json(),
+                   "nocache": reference.run_nocache(jpath, max_size), "ltl_bs": {}}
+            for rlx in rlx_types:
+                rec["ltl_bs"][str(rlx)] = reference.run_ltl_bs(tpath, max_size, rlx)
+            runs.append(rec)
+            print(name, rec["nocache"]["formula"],
+                  {k: v["formula"] for k, v in rec["ltl_bs"].items()}, flush=True)
+    with open(OUT, "w") as f:
+        json.dump({"generated_by": "tests/golden/make_goldens.py", "instances": runs}, f, indent=1)
+    print("wrote", OUT)
+
+
+if __name__ == "__main__":
+    main()

@@ -16,7 +16,8 @@ constexpr int kMaxSize = 32;          // formula size limit (ltl_nocache.cu:11)
 constexpr int kMaxSplits = 16;        // floor((32-1)/2)
 constexpr int kGroups = 1 + kMaxSplits;
 constexpr int kTS = 128;              // stream rows per P1 tile (= threads per CTA)
-constexpr int kTQ = 32;               // staged rows per P1 tile
+constexpr int kTQ = 32;               // staged rows per P1 tile (maximum)
+constexpr int kP1TileTarget = 1024;   // shrink the staged height until a level has this many tiles
 constexpr int kMaxProbes = 4096;      // bounded linear probing
 constexpr uint64_t kEmpty = ~0ULL;
 constexpr int kPayShift = 58;         // payload = level << 58 | candidate index
@@ -80,6 +81,8 @@ struct InstDev {
   // P1 tile groups: group 0 = unary over level k-1, group s = split s
   uint64_t grp_prefix[kGroups + 1];
   uint32_t grp_qtiles[kGroups];
+  int tq;                      // staged rows per P1 tile at this level (1..kTQ)
+  int pad1;
   // per-level counters
   unsigned long long n_tent, n_new, n_wins, probe_fail;
   unsigned long long best_sol;  // min candidate index of a solution winner

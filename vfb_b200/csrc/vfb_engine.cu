@@ -263,7 +263,7 @@ struct Engine {
 
   // --------------------------------------------------------- step launch
   void launch_step(int ninst, int p1_smem, bool timed) {
-    const int g = grid;
+    const int g = grid, gc = sms * 2;
     int e = 0;
     auto mark = [&]() { if (timed) cudaEventRecord(ev_k[e++], stream); };
     mark();
@@ -276,11 +276,11 @@ struct Engine {
         k_verify<<<g, 256, 0, stream>>>(dB);
         mark();
       }
-      k_chunk_count<<<g, 256, 0, stream>>>(dB, phase);
+      k_chunk_count<<<gc, 256, 0, stream>>>(dB, phase);
       mark();
       k_chunk_scan<<<std::min(ninst, g), kScanThreads, 0, stream>>>(dB, phase);
       mark();
-      k_chunk_emit<<<g, kChunkThreads, 0, stream>>>(dB, phase);
+      k_chunk_emit<<<gc, kChunkThreads, 0, stream>>>(dB, phase);
       mark();
     }
     k_emit_rows<<<g, 256, 0, stream>>>(dB);
@@ -339,7 +339,7 @@ struct Engine {
     if (!loop) {
       e = cudaStreamBeginCaptureToGraph(stream, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
       if (e != cudaSuccess) { cudaGraphDestroy(graph); return e; }
-      launch_step(ninst, p1_smem, profile != 0);
+      launch_step(ninst, p1_smem, false);
       cudaMemcpyAsync(h_status, hB.status_out, (size_t)ninst * sizeof(int2), cudaMemcpyDeviceToHost, stream);
       cudaGraph_t out = nullptr;
       e = cudaStreamEndCapture(stream, &out);
@@ -356,6 +356,14 @@ struct Engine {
   }
 
   cudaError_t run(int ninst, int p1_smem) {
+    if (profile) {
+      // per-kernel CUDA events need plain launches (events recorded during
+      // stream capture only order the capture, they take no timestamps)
+      launch_step(ninst, p1_smem, true);
+      c_d2h += (uint64_t)ninst * sizeof(int2);
+      return cudaMemcpyAsync(h_status, hB.status_out, (size_t)ninst * sizeof(int2), cudaMemcpyDeviceToHost,
+                             stream);
+    }
     if (!exec || exec_ninst != ninst || exec_smem != p1_smem || exec_grid != p1_grid ||
         exec_loop != (int)use_loop) {
       const cudaError_t e = build_graph(ninst, p1_smem);

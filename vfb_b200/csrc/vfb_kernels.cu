@@ -248,20 +248,29 @@ __global__ void k_plan(BatchDev* Bp) {
       I.base_g = g; g += n[k - 1];
       for (int i = 1; i <= k - 2; ++i) { I.base_u[i] = g; g += n[i] * n[k - 1 - i]; }
       I.cands = g;
-      uint64_t t = (n[k - 1] + kTS - 1) / kTS;
-      I.grp_prefix[0] = 0;
-      I.grp_prefix[1] = t;
-      for (int i = 1; i < kGroups; ++i) {
-        if (2 * i <= k - 1) {
-          const int j = k - 1 - i;
-          const bool qleft = (i == j) || (n[i] <= n[j]);
-          const uint64_t nS = qleft ? n[j] : n[i], nQ = qleft ? n[i] : n[j];
-          const uint64_t qt = (nQ + kTQ - 1) / kTQ, st = (nS + kTS - 1) / kTS;
-          I.grp_qtiles[i] = (uint32_t)qt;
-          t += st * qt;
+      // P1 tiling: kTS stream rows x tq staged rows per tile; small levels get
+      // shorter tiles so that they still spread over every SM
+      uint64_t t = 0;
+      int tq = kTQ;
+      for (;;) {
+        t = (n[k - 1] + kTS - 1) / kTS;
+        I.grp_prefix[0] = 0;
+        I.grp_prefix[1] = t;
+        for (int i = 1; i < kGroups; ++i) {
+          if (2 * i <= k - 1) {
+            const int j = k - 1 - i;
+            const bool qleft = (i == j) || (n[i] <= n[j]);
+            const uint64_t nS = qleft ? n[j] : n[i], nQ = qleft ? n[i] : n[j];
+            const uint64_t qt = (nQ + tq - 1) / tq, st = (nS + kTS - 1) / kTS;
+            I.grp_qtiles[i] = (uint32_t)qt;
+            t += st * qt;
+          }
+          I.grp_prefix[i + 1] = t;
         }
-        I.grp_prefix[i + 1] = t;
+        if (t >= (uint64_t)kP1TileTarget || tq == 1) break;
+        tq >>= 1;
       }
+      I.tq = tq;
       const uint64_t words = (g + 31) / 32;
       const uint64_t cap = I.table_mask + 1;
       // new keys of this level: at most all candidates; expect ~8x growth
@@ -306,7 +315,7 @@ struct TileSh {
   uint64_t s0, q0, nS, nQ, ni, nj;
   int si, qi;   // levels of the stream / staged operand
   int qleft;    // staged operand is the left operand of & | and of U(i->j)
-  int i, j;
+  int i, j, tq;
   uint8_t len[kMaxTraces], off[kMaxTraces], wid[kMaxTraces];
 };
 
@@ -384,7 +393,7 @@ __device__ void p1_binary(InstDev& I, const TileSh& P, const uint64_t* sS, int s
   const uint64_t s = P.s0 + threadIdx.x;
   if (s >= P.nS) return;
   const uint64_t* srow = sS + threadIdx.x * sp;
-  const int nq = (int)((P.nQ - P.q0) < (uint64_t)kTQ ? (P.nQ - P.q0) : (uint64_t)kTQ);
+  const int nq = (int)((P.nQ - P.q0) < (uint64_t)P.tq ? (P.nQ - P.q0) : (uint64_t)P.tq);
   for (int q = 0; q < nq; ++q) {
     const uint64_t* qrow = sQ + q * P.TP;
     KeyAcc kA, kO, kU, kV;
@@ -443,6 +452,7 @@ __global__ void __launch_bounds__(kTS) k_p1(BatchDev* Bp) {
         P.half = I.T / 2;
         P.stride = I.stride1;
         P.mode = I.key_mode;
+        P.tq = I.tq;
         // give up early once the table is known to be too small for this level
         const unsigned long long cap = I.table_mask + 1;
         P.skip = (*(volatile unsigned long long*)&I.probe_fail != 0) ||
@@ -467,7 +477,7 @@ __global__ void __launch_bounds__(kTS) k_p1(BatchDev* Bp) {
           P.nQ = qleft ? ni : nj;
           const uint64_t qt = I.grp_qtiles[grp];
           P.s0 = (within / qt) * kTS;
-          P.q0 = (within % qt) * kTQ;
+          P.q0 = (within % qt) * I.tq;
         }
       }
     }
@@ -487,7 +497,7 @@ __global__ void __launch_bounds__(kTS) k_p1(BatchDev* Bp) {
       const int ns = (int)((P.nS - P.s0) < (uint64_t)kTS ? (P.nS - P.s0) : (uint64_t)kTS);
       stage_rows(sS, sp, row_ptr(I, P.si, P.s0), ns, P.TP);
       if (P.grp > 0) {
-        const int nq = (int)((P.nQ - P.q0) < (uint64_t)kTQ ? (P.nQ - P.q0) : (uint64_t)kTQ);
+        const int nq = (int)((P.nQ - P.q0) < (uint64_t)P.tq ? (P.nQ - P.q0) : (uint64_t)P.tq);
         stage_rows(sQ, P.TP, row_ptr(I, P.qi, P.q0), nq, P.TP);
       }
     }
@@ -640,9 +650,12 @@ __global__ void k_chunk_scan(BatchDev* Bp, int phase) {
 }
 
 // Emit set bits of each chunk in order; always clears the chunk's words.
+// The chunk is loaded coalesced into shared memory (padded rows of 16 words),
+// then every thread scans its 16 consecutive words.
 __global__ void __launch_bounds__(kChunkThreads) k_chunk_emit(BatchDev* Bp, int phase) {
   __shared__ unsigned long long s_w[32];
   constexpr int kPer = kChunkWords / kChunkThreads;   // 16 words per thread
+  __shared__ uint32_t s_bits[kChunkThreads * (kPer + 1)];
   const BatchDev B = *Bp;
   const unsigned long long* prefix = phase ? B.chunk_prefix1 : B.chunk_prefix0;
   const unsigned long long total = prefix[B.ninst];
@@ -650,31 +663,31 @@ __global__ void __launch_bounds__(kChunkThreads) k_chunk_emit(BatchDev* Bp, int 
     const int b = find_owner(prefix, B.ninst, c);
     InstDev& I = B.inst[b];
     const uint64_t words = (phase_bits(I, phase) + 31) / 32;
-    const uint64_t wbeg = (c - prefix[b]) * kChunkWords + (uint64_t)threadIdx.x * kPer;
-    uint32_t mine[kPer];
+    const uint64_t cbeg = (c - prefix[b]) * kChunkWords;
+    for (int u = threadIdx.x; u < kChunkWords; u += blockDim.x) {
+      const uint64_t w = cbeg + u;
+      const uint32_t v = (w < words) ? I.bitmap[w] : 0u;
+      s_bits[(u / kPer) * (kPer + 1) + (u % kPer)] = v;
+      if (v) I.bitmap[w] = 0u;
+    }
+    __syncthreads();
+    const uint32_t* mine = s_bits + threadIdx.x * (kPer + 1);
     unsigned long long cnt = 0;
 #pragma unroll
-    for (int u = 0; u < kPer; ++u) {
-      const uint64_t w = wbeg + u;
-      mine[u] = (w < words) ? I.bitmap[w] : 0u;
-      cnt += __popc(mine[u]);
-    }
+    for (int u = 0; u < kPer; ++u) cnt += __popc(mine[u]);
     unsigned long long tot;
     unsigned long long pos = block_excl_scan(cnt, s_w, tot) + B.chunk_base[c];
-    const bool run = I.status == ST_RUNNING;
-    uint64_t* out = phase ? I.wins : I.tent;
-#pragma unroll
-    for (int u = 0; u < kPer; ++u) {
-      const uint64_t w = wbeg + u;
-      if (w >= words) continue;
-      uint32_t bits = mine[u];
-      if (bits) I.bitmap[w] = 0u;
-      if (!run) continue;
-      while (bits) {
-        const int p = __ffs(bits) - 1;
-        bits &= bits - 1;
-        const uint64_t idx = w * 32 + p;
-        out[pos++] = phase ? I.tent[idx] : idx;
+    if (I.status == ST_RUNNING && cnt) {
+      uint64_t* out = phase ? I.wins : I.tent;
+      const uint64_t wbeg = cbeg + (uint64_t)threadIdx.x * kPer;
+      for (int u = 0; u < kPer; ++u) {
+        uint32_t bits = mine[u];
+        while (bits) {
+          const int p = __ffs(bits) - 1;
+          bits &= bits - 1;
+          const uint64_t idx = (wbeg + u) * 32 + p;
+          out[pos++] = phase ? I.tent[idx] : idx;
+        }
       }
     }
     __syncthreads();
