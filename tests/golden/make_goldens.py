@@ -27,6 +27,14 @@ from vfb_b200 import synth  # noqa: E402
 
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_runs.json")
 
+# LTL_BS runs that aborted (exit -6 after a CUDA error, at the first cost with
+# a solution) when this fixture was made.  Reading LTL_BS.cu shows why: the
+# U launch compacts 2N temp slots of which only N were written (1465-1482), so
+# stale or never-written slots enter the cache with arbitrary parent indices,
+# and the reconstruction kernel (generateResIndices 561-587) follows them out
+# of bounds.  They are recorded in the fixture and never run again.
+FAULTED = {("relaxed2", 1), ("relaxed2", 2), ("relaxed2", 3), ("relaxed5", 2)}
+
 
 def instances():
     out = []
@@ -58,6 +66,11 @@ def main():
     if not reference.build_if_present():
         if not reference.available():
             raise SystemExit("reference programs are not built (oracle/_ref)")
+    previous = {}
+    if os.path.exists(OUT):
+        for r in json.load(open(OUT))["instances"]:
+            for k, v in r["ltl_bs"].items():
+                previous[(r["name"], k)] = v
     runs = []
     with tempfile.TemporaryDirectory() as tmp:
         for idx, (inst, max_size, rlx_types) in enumerate(instances()):
@@ -70,6 +83,9 @@ def main():
             rec = {"name": name, "max_size": max_size, "json": inst.to_json(),
                    "nocache": reference.run_nocache(jpath, max_size), "ltl_bs": {}}
             for rlx in rlx_types:
+                if (name, rlx) in FAULTED:
+                    rec["ltl_bs"][str(rlx)] = previous.get((name, str(rlx)))
+                    continue
                 rec["ltl_bs"][str(rlx)] = reference.run_ltl_bs(tpath, max_size, rlx)
             runs.append(rec)
             print(name, rec["nocache"]["formula"],
