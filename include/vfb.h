@@ -100,6 +100,27 @@ vfb_status vfb_solve(void *ctx, const vfb_instance *inst, vfb_result *out);
 /* Solves n independent instances together; out[i] equals vfb_solve(inst[i]). */
 vfb_status vfb_batch_solve(void *ctx, const vfb_instance *inst, int n, vfb_result *out);
 
+/* Solve without allocating.  No counterpart in the reference.
+ *
+ * For callers that may not allocate device (or pinned host) memory while they
+ * run -- a process whose device heap is owned by another allocator, a
+ * latency-critical loop that cannot take cudaMalloc's implicit
+ * synchronisation, a driver heap closed after start-up.  Needs no context:
+ * it runs the same kernels as vfb_solve on the current device and the legacy
+ * default stream, with every device buffer carved from one static array of
+ * VFB_NOALLOC_SCRATCH_BYTES that the library's module holds on every GPU that
+ * loads it, until the process exits.  Buffers do not grow: the array holds a
+ * hash set of 2^19 slots (kept at most half full), a bitmap of 2^25 candidates
+ * per size, 2^19 tentative and winner entries, and about 36 MiB of level cache
+ * (for 40 traces, about 110000 characteristic sets); a search that needs more
+ * stops with VFB_OOM and a message on stderr.  The first call on a device resolves the array's
+ * address and should come before any stream capture.  All calls share the
+ * array (each one clears what must start empty); calls that overlap on the
+ * GPU race, so serialise them.  Results equal vfb_solve's for every instance
+ * that fits; device_seconds is not measured (0). */
+#define VFB_NOALLOC_SCRATCH_BYTES (64u << 20)
+vfb_status vfb_solve_noalloc(const vfb_instance *inst, vfb_result *out);
+
 /* Per-kernel profile accumulated since vfb_create (profile=1 only).  name,
  * number of launches, total device milliseconds (CUDA events around each
  * launch) and the algorithmic bytes those launches had to move (operand rows

@@ -68,7 +68,7 @@ class _JsonProblem(ctypes.Structure):
 
 EXPORTS = ["vfb_create", "vfb_destroy", "vfb_solve", "vfb_batch_solve", "vfb_status_str",
            "vfb_read_json", "vfb_json_free", "vfb_format_infix", "vfb_profile_read",
-           "vfb_profile_reset"]
+           "vfb_profile_reset", "vfb_solve_noalloc"]
 
 _lib = None
 
@@ -108,6 +108,8 @@ def load_library():
     lib.vfb_profile_read.restype = ctypes.c_int
     lib.vfb_profile_reset.argtypes = [ctypes.c_void_p]
     lib.vfb_profile_reset.restype = None
+    lib.vfb_solve_noalloc.argtypes = [ctypes.POINTER(_Instance), ctypes.POINTER(_Result)]
+    lib.vfb_solve_noalloc.restype = ctypes.c_int
     _lib = lib
     return lib
 
@@ -270,6 +272,17 @@ class Engine:
         if rc not in (OK, NOT_FOUND):
             raise VfbError(f"vfb_batch_solve failed: {STATUS_NAMES[rc]}")
         return [_result(res[i]) for i in range(n)]
+
+
+def solve_noalloc(prob: Problem) -> Result:
+    """vfb_solve_noalloc: the solve without any allocation (static scratch of
+    VFB_NOALLOC_SCRATCH_BYTES on the current device; VFB_OOM if it does not fit)."""
+    lib = load_library()
+    inst, keep = prob._cstruct()
+    res = _Result()
+    lib.vfb_solve_noalloc(ctypes.byref(inst), ctypes.byref(res))
+    del keep
+    return _result(res)
 
 
 def ltl(max_len: int, input_data, trace_len, num_vars: int, num_pos: int, names,
