@@ -75,6 +75,8 @@ struct Engine {
   int p1_grid = 0;     // P1 CTAs
   cudaError_t last_error = cudaSuccess;
   bool use_loop = true;  // device-side while-node available
+  bool use_coop = true;  // persistent cooperative solver (k_solve)
+  int coop_grid = 0;
 
   // batch workspace
   int ninst_cap = 0;
@@ -82,6 +84,7 @@ struct Engine {
   BatchDev* dB = nullptr;
   InstDev* dInst = nullptr;
   int2* h_status = nullptr;   // pinned mirror of B.status_out
+  unsigned int* h_ctl = nullptr;  // pinned mirror of B.ctl
   unsigned long long* d_fail = nullptr;
   uint64_t* h_stage = nullptr;  // pinned upload staging
   size_t h_stage_words = 0;
@@ -118,6 +121,8 @@ struct Engine {
     h_stage = nullptr;
     if (d_fail) cudaFree(d_fail);
     d_fail = nullptr;
+    if (h_ctl) cudaFreeHost(h_ctl);
+    h_ctl = nullptr;
     if (ev_t0) cudaEventDestroy(ev_t0);
     if (ev_t1) cudaEventDestroy(ev_t1);
     for (auto& e : ev_k)
@@ -129,7 +134,8 @@ struct Engine {
   void free_workspace() {
     auto f = [&](void* p) { if (p) cudaFree(p); };
     f(hB.p1_prefix); f(hB.chunk_prefix0); f(hB.chunk_prefix1); f(hB.tent_prefix); f(hB.win_prefix);
-    f(hB.chunk_cnt); f(hB.chunk_base); f(hB.tickets); f(hB.status_out); f(hB.loop_iter); f(dB); f(dInst);
+    f(hB.chunk_cnt); f(hB.chunk_base); f(hB.tickets); f(hB.status_out); f(hB.loop_iter); f(hB.ctl); f(dB);
+    f(dInst);
     hB = BatchDev{};
     dB = nullptr;
     dInst = nullptr;
@@ -137,12 +143,13 @@ struct Engine {
   }
 
   // ------------------------------------------------------ device blocks
-  // Returns a block of at least `bytes`; *got is its real size.  Cached blocks
-  // up to 4x the request are reused (their full size becomes the capacity).
+  // Returns a block of at least `bytes`; *got is its real size.  The smallest
+  // cached block that fits is reused and its full size becomes the capacity,
+  // so a repeated solve starts with the buffers its predecessor grew.
   void* dalloc(size_t bytes, size_t* got) {
     if (bytes < 256) bytes = 256;
     auto it = free_blocks.lower_bound(bytes);
-    if (it != free_blocks.end() && it->first <= 4 * bytes) {
+    if (it != free_blocks.end()) {
       void* p = it->second;
       *got = it->first;
       free_blocks.erase(it);
@@ -200,6 +207,7 @@ struct Engine {
       cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
     }
     if (cudaMalloc(&d_fail, sizeof(unsigned long long)) != cudaSuccess) return VFB_DEVICE_ERROR;
+    if (cudaMallocHost(&h_ctl, 4 * sizeof(unsigned int)) != cudaSuccess) return VFB_DEVICE_ERROR;
     if (cudaEventCreate(&ev_t0) != cudaSuccess || cudaEventCreate(&ev_t1) != cudaSuccess) return VFB_DEVICE_ERROR;
     for (auto& e : ev_k)
       if (cudaEventCreate(&e) != cudaSuccess) return VFB_DEVICE_ERROR;
@@ -209,8 +217,17 @@ struct Engine {
       return VFB_DEVICE_ERROR;
     cudaFuncAttributes fa;
     if (cudaFuncGetAttributes(&fa, k_p1) != cudaSuccess) return VFB_DEVICE_ERROR;
+    if (cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsmem) != cudaSuccess)
+      return VFB_DEVICE_ERROR;
     const char* env = std::getenv("VFB_NO_DEVICE_LOOP");
     use_loop = !(env && env[0] == '1') && !profile;
+    // level loop: persistent cooperative kernel unless profiling per kernel,
+    // the device cannot co-schedule a grid, or VFB_SOLVER=graph asks otherwise
+    int coop = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+    const char* sol = std::getenv("VFB_SOLVER");
+    use_coop = coop && !profile && !(sol && std::strcmp(sol, "graph") == 0) &&
+               !(env && env[0] == '1');
     return VFB_OK;
   }
 
@@ -236,7 +253,9 @@ struct Engine {
       WS_ALLOC(tickets, 4 * sizeof(unsigned long long))
       WS_ALLOC(status_out, (size_t)nc * sizeof(int2))
       WS_ALLOC(loop_iter, sizeof(unsigned long long))
+      WS_ALLOC(ctl, 4 * sizeof(unsigned int))
 #undef WS_ALLOC
+      cudaMemset(nb.ctl, 0, 4 * sizeof(unsigned int));
       BatchDev* ndB = nullptr;
       if (cudaMalloc((void**)&ndB, sizeof(BatchDev)) != cudaSuccess) return VFB_OOM;
       InstDev* ndI = nullptr;
@@ -265,7 +284,8 @@ struct Engine {
   void launch_step(int ninst, int p1_smem, bool timed) {
     const int g = grid, gc = sms * 2;
     int e = 0;
-    auto mark = [&]() { if (timed) cudaEventRecord(ev_k[e++], stream); };
+    // external event nodes keep their timestamps inside a captured graph
+    auto mark = [&]() { if (timed) cudaEventRecordWithFlags(ev_k[e++], stream, cudaEventRecordExternal); };
     mark();
     k_plan<<<1, 1024, 0, stream>>>(dB);
     mark();
@@ -339,7 +359,7 @@ struct Engine {
     if (!loop) {
       e = cudaStreamBeginCaptureToGraph(stream, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
       if (e != cudaSuccess) { cudaGraphDestroy(graph); return e; }
-      launch_step(ninst, p1_smem, false);
+      launch_step(ninst, p1_smem, profile != 0);
       cudaMemcpyAsync(h_status, hB.status_out, (size_t)ninst * sizeof(int2), cudaMemcpyDeviceToHost, stream);
       cudaGraph_t out = nullptr;
       e = cudaStreamEndCapture(stream, &out);
@@ -356,13 +376,21 @@ struct Engine {
   }
 
   cudaError_t run(int ninst, int p1_smem) {
-    if (profile) {
-      // per-kernel CUDA events need plain launches (events recorded during
-      // stream capture only order the capture, they take no timestamps)
-      launch_step(ninst, p1_smem, true);
-      c_d2h += (uint64_t)ninst * sizeof(int2);
-      return cudaMemcpyAsync(h_status, hB.status_out, (size_t)ninst * sizeof(int2), cudaMemcpyDeviceToHost,
-                             stream);
+    if (use_coop) {
+      if (coop_grid <= 0) return cudaErrorInvalidConfiguration;
+      const unsigned int init_ctl[2] = {0u, 1u};   // error, continue
+      cudaMemcpyAsync(hB.ctl + 2, init_ctl, sizeof(init_ctl), cudaMemcpyHostToDevice, stream);
+      cudaMemsetAsync(hB.loop_iter, 0, sizeof(unsigned long long), stream);
+      unsigned int steps = kMaxLoop;
+      void* args[] = {(void*)&dB, (void*)&steps};
+      cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_solve, dim3(coop_grid), dim3(kTS), args,
+                                                  (size_t)p1_smem, stream);
+      if (e != cudaSuccess) return e;
+      cudaMemcpyAsync(h_status, hB.status_out, (size_t)ninst * sizeof(int2), cudaMemcpyDeviceToHost, stream);
+      cudaMemcpyAsync(h_ctl, hB.ctl, 4 * sizeof(unsigned int), cudaMemcpyDeviceToHost, stream);
+      c_h2d += sizeof(init_ctl);
+      c_d2h += (uint64_t)ninst * sizeof(int2) + 4 * sizeof(unsigned int);
+      return cudaSuccess;
     }
     if (!exec || exec_ninst != ninst || exec_smem != p1_smem || exec_grid != p1_grid ||
         exec_loop != (int)use_loop) {
@@ -636,6 +664,10 @@ struct Engine {
     int occ = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_p1, kTS, p1_smem);
     p1_grid = sms * std::max(occ, 1);
+    int occ2 = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k_solve, kTS, p1_smem);
+    coop_grid = sms * occ2;
+    if (coop_grid <= 0) use_coop = false;
 
     vfb_status rc = VFB_OK;
     uint64_t chunk_need = 0;
@@ -713,8 +745,13 @@ struct Engine {
       cudaError_t e = run(n, p1_smem);
       if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
       if (e != cudaSuccess) { last_error = e; rc = VFB_DEVICE_ERROR; break; }
-      c_launch += exec_loop ? 0 : (uint64_t)kStepLen;
-      if (exec_loop) {
+      if (use_coop) {
+        c_launch += 1;
+        if (h_ctl[2] != 0) { rc = VFB_DEVICE_ERROR; break; }
+      } else {
+        c_launch += exec_loop ? 0 : (uint64_t)kStepLen;
+      }
+      if (!use_coop && exec_loop) {
         unsigned long long it = 0;
         cudaMemcpy(&it, hB.loop_iter, sizeof(it), cudaMemcpyDeviceToHost);
         c_d2h += sizeof(it);

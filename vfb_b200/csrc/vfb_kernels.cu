@@ -24,214 +24,13 @@
 // The reference's thrust::remove/copy_n compaction (storeUniqueLTLs
 // LTL_BS.cu:489-530) is replaced by the bitmap compaction; its racy
 // atomicCAS winners (LTL_BS.cu:319, hash_set.cuh:232) by min-index ownership.
-#include "vfb_kernels.cuh"
+#include "vfb_ops.cuh"
 
 namespace vfb {
 
-// ------------------------------------------------------------------ helpers
-__device__ __forceinline__ Key128 ld_key(const Slot* s) {
-  const ulonglong2 v = __ldcg(reinterpret_cast<const ulonglong2*>(s));
-  return Key128{v.x, v.y};
-}
-
-__device__ __forceinline__ unsigned long long pay_of(int k, uint64_t g) {
-  return ((unsigned long long)k << kPayShift) | (unsigned long long)g;
-}
-
-// Lower the key's payload to pay.  Returns 1 when pay is the key's minimum
-// after the update (the candidate may own the key), 0 otherwise.  A payload
-// equal to pay means the same candidate claimed it in an earlier attempt of
-// this level, which still counts as owning.
-__device__ __forceinline__ int claim(Slot* s, unsigned long long pay) {
-  const unsigned long long cur = __ldcg(&s->pay);
-  if (cur < pay) return 0;
-  if (cur == pay) return 1;
-  const unsigned long long old = atomicMin(&s->pay, pay);
-  return old >= pay ? 1 : 0;
-}
-
-// Insert-or-find (h,l) starting at slot idx whose key half-words were already
-// loaded into cur.  Returns 1/0 as claim(), -1 when the probe limit is hit.
-__device__ int insert_min(Slot* tab, uint64_t mask, uint64_t idx, Key128 cur, uint64_t h, uint64_t l,
-                          unsigned long long pay, int& isnew) {
-  for (int p = 0; p < kMaxProbes; ++p) {
-    if (p > 0) cur = ld_key(tab + idx);
-    if (cur.h == h && cur.l == l) return claim(tab + idx, pay);
-    // A real key never has a half equal to ~0 (normalised away), so a ~0 half
-    // is either an empty slot or a key being published: resolve with the CAS.
-    if (cur.h == kEmpty || cur.l == kEmpty) {
-      const Key128 old = atomicCAS(reinterpret_cast<Key128*>(tab + idx), Key128{kEmpty, kEmpty},
-                                   Key128{h, l});
-      if (old.h == kEmpty && old.l == kEmpty) {
-        isnew = 1;
-        return claim(tab + idx, pay);
-      }
-      if (old.h == h && old.l == l) return claim(tab + idx, pay);
-    }
-    idx = (idx + 1) & mask;
-  }
-  return -1;
-}
-
-// Payload of (h,l), or ~0 if the key is absent.
-__device__ unsigned long long find_pay(const Slot* tab, uint64_t mask, uint64_t h, uint64_t l) {
-  uint64_t idx = slot_hash(h, l) & mask;
-  for (int p = 0; p < kMaxProbes; ++p) {
-    const Key128 cur = ld_key(tab + idx);
-    if (cur.h == h && cur.l == l) return __ldcg(&tab[idx].pay);
-    if (cur.h == kEmpty && cur.l == kEmpty) return ~0ULL;
-    idx = (idx + 1) & mask;
-  }
-  return ~0ULL;
-}
-
-// Largest b with prefix[b] <= x (prefix non-decreasing, prefix[0] = 0 <= x < prefix[n]).
-__device__ __forceinline__ int find_owner(const unsigned long long* prefix, int n, unsigned long long x) {
-  int lo = 0, hi = n;  // prefix[lo] <= x < prefix[hi]
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (prefix[mid] <= x) lo = mid; else hi = mid;
-  }
-  return lo;
-}
-
-template <typename V>
-__device__ __forceinline__ V warp_sum(V v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  return v;
-}
-
-// Block-wide exclusive scan of one value per thread (blockDim multiple of 32).
-__device__ unsigned long long block_excl_scan(unsigned long long v, unsigned long long* s_warp,
-                                              unsigned long long& total) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  unsigned long long x = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) s_warp[wid] = x;
-  __syncthreads();
-  if (wid == 0) {
-    unsigned long long w = lane < nw ? s_warp[lane] : 0ULL;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const unsigned long long y = __shfl_up_sync(0xffffffffu, w, o);
-      if (lane >= o) w += y;
-    }
-    if (lane < nw) s_warp[lane] = w;
-  }
-  __syncthreads();
-  total = s_warp[nw - 1];
-  const unsigned long long before = wid > 0 ? s_warp[wid - 1] : 0ULL;
-  __syncthreads();
-  return before + x - v;
-}
-
-__device__ __forceinline__ uint64_t apply_w(int op, uint64_t l, uint64_t r, int L) {
-  switch (op) {
-    case OP_NOT: return ~l & len_mask(L);
-    case OP_AND: return l & r;
-    case OP_OR: return l | r;
-    case OP_X: return l >> 1;
-    case OP_F: return w_fin(l);
-    case OP_G: return w_glob(l, len_mask(L));
-    default: return w_until(l, r);
-  }
-}
-
-struct Cand {
-  int op, la, lb;
-  uint64_t a, b;
-};
-
-// Canonical candidate index g of level k -> operator and operands (levels and
-// indices within them).  Block order ~ & | X F G U; & and | over left sizes
-// 1..floor((k-1)/2), U over 1..k-2; left index major (ltl_nocache.cu:169-224).
-__device__ Cand decode(const InstDev& I, int k, uint64_t g) {
-  const uint64_t* n = I.lcount;
-  Cand c;
-  c.lb = 0;
-  c.b = 0;
-  const uint64_t un = n[k - 1];
-  if (g < un) { c.op = OP_NOT; c.la = k - 1; c.a = g; return c; }
-  g -= un;
-  for (int pass = 0; pass < 2; ++pass) {
-    for (int i = 1; 2 * i <= k - 1; ++i) {
-      const int j = k - 1 - i;
-      const uint64_t cnt = n[i] * n[j];
-      if (g < cnt) {
-        c.op = pass ? OP_OR : OP_AND;
-        c.la = i; c.lb = j; c.a = g / n[j]; c.b = g % n[j];
-        return c;
-      }
-      g -= cnt;
-    }
-  }
-  for (int op = OP_X; op <= OP_G; ++op) {
-    if (g < un) { c.op = op; c.la = k - 1; c.a = g; return c; }
-    g -= un;
-  }
-  for (int i = 1; i <= k - 2; ++i) {
-    const int j = k - 1 - i;
-    const uint64_t cnt = n[i] * n[j];
-    if (g < cnt) {
-      c.op = OP_U; c.la = i; c.lb = j; c.a = g / n[j]; c.b = g % n[j];
-      return c;
-    }
-    g -= cnt;
-  }
-  c.op = -1;
-  c.la = 1;
-  c.a = 0;
-  return c;
-}
-
-__device__ __forceinline__ const uint64_t* row_ptr(const InstDev& I, int lvl, uint64_t idx) {
-  return I.rows + (I.lstart[lvl] + idx) * (uint64_t)I.TP;
-}
-
-template <int MODE>
-__device__ void cand_key(const InstDev& I, const Cand& c, uint64_t& h, uint64_t& l) {
-  const uint64_t* ra = row_ptr(I, c.la, c.a);
-  const uint64_t* rb = (c.op == OP_AND || c.op == OP_OR || c.op == OP_U) ? row_ptr(I, c.lb, c.b) : ra;
-  KeyAcc k;
-  key_init(k);
-  const int T = I.T, half = T / 2;
-  for (int t = 0; t < T; ++t) {
-    const uint64_t w = apply_w(c.op, ra[t], rb[t], I.len[t]);
-    key_word<MODE>(k, w, t, half, I.off[t], I.width[t], I.stride1, I.len[t]);
-  }
-  key_final<MODE>(k, h, l);
-}
-
-__device__ void row_key(const InstDev& I, const uint64_t* row, uint64_t& h, uint64_t& l) {
-  KeyAcc k;
-  key_init(k);
-  const int T = I.T, half = T / 2;
-  switch (I.key_mode) {
-    case KEY_HASH:
-      for (int t = 0; t < T; ++t) key_word<KEY_HASH>(k, row[t], t, half, 0, 0, 0, 0);
-      key_final<KEY_HASH>(k, h, l);
-      break;
-    case KEY_SAMPLED:
-      for (int t = 0; t < T; ++t)
-        key_word<KEY_SAMPLED>(k, row[t], t, half, I.off[t], I.width[t], I.stride1, I.len[t]);
-      key_final<KEY_SAMPLED>(k, h, l);
-      break;
-    default:
-      for (int t = 0; t < T; ++t)
-        key_word<KEY_CONCAT>(k, row[t], t, half, I.off[t], I.width[t], 0, I.len[t]);
-      key_final<KEY_CONCAT>(k, h, l);
-  }
-}
-
 // ===================================================================== plan
-__global__ void k_plan(BatchDev* Bp) {
-  const BatchDev B = *Bp;
-  for (int b = threadIdx.x; b < B.ninst; b += blockDim.x) {
+__device__ void ph_plan(const BatchDev& B, unsigned bid, unsigned nb) {
+  for (int b = bid * blockDim.x + threadIdx.x; b < B.ninst; b += nb * blockDim.x) {
     InstDev& I = B.inst[b];
     unsigned long long tiles = 0, chunks = 0;
     if (I.status == ST_RUNNING) {
@@ -295,143 +94,32 @@ __global__ void k_plan(BatchDev* Bp) {
     B.p1_prefix[b + 1] = tiles;
     B.chunk_prefix0[b + 1] = chunks;
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    B.p1_prefix[0] = 0;
-    B.chunk_prefix0[0] = 0;
-    for (int b = 0; b < B.ninst; ++b) {
-      B.p1_prefix[b + 1] += B.p1_prefix[b];
-      B.chunk_prefix0[b + 1] += B.chunk_prefix0[b];
-    }
-    for (int i = 0; i < 4; ++i) B.tickets[i] = 0;
+}
+
+// One thread: cross-instance prefixes of P1 tiles and bitmap chunks; resets
+// the work tickets of the step.
+__device__ void ph_plan_prefix(const BatchDev& B) {
+  B.p1_prefix[0] = 0;
+  B.chunk_prefix0[0] = 0;
+  for (int b = 0; b < B.ninst; ++b) {
+    B.p1_prefix[b + 1] += B.p1_prefix[b];
+    B.chunk_prefix0[b + 1] += B.chunk_prefix0[b];
   }
+  for (int i = 0; i < 4; ++i) B.tickets[i] = 0;
+}
+
+__global__ void k_plan(BatchDev* Bp) {
+  const BatchDev B = *Bp;
+  ph_plan(B, 0, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) ph_plan_prefix(B);
 }
 
 // ======================================================================= P1
-// Shared per-tile parameters.
-struct TileSh {
-  unsigned long long tile;
-  int inst, grp, k, T, TP, half, stride, mode, skip;
-  uint64_t s0, q0, nS, nQ, ni, nj;
-  int si, qi;   // levels of the stream / staged operand
-  int qleft;    // staged operand is the left operand of & | and of U(i->j)
-  int i, j, tq;
-  uint8_t len[kMaxTraces], off[kMaxTraces], wid[kMaxTraces];
-};
-
-// Copy nrows consecutive rows (pitch TP words, 16-byte aligned) into shared
-// memory with pitch sp, as 128-bit coalesced loads.
-__device__ __forceinline__ void stage_rows(uint64_t* dst, int sp, const uint64_t* src, int nrows, int TP) {
-  const int n2 = nrows * TP / 2;
-  const ulonglong2* s2 = reinterpret_cast<const ulonglong2*>(src);
-  for (int u = threadIdx.x; u < n2; u += blockDim.x) {
-    const ulonglong2 v = __ldg(s2 + u);
-    const int w = 2 * u, r = w / TP, c = w - r * TP;
-    dst[r * sp + c] = v.x;
-    dst[r * sp + c + 1] = v.y;
-  }
-}
-
-struct P1Count {
-  unsigned long long tent, fresh, fail;
-};
-
-template <int N>
-__device__ __forceinline__ void insert_group(InstDev& I, Slot* tab, uint64_t mask, int k, const uint64_t* h,
-                                             const uint64_t* l, const uint64_t* g, P1Count& cnt) {
-  uint64_t idx[N];
-  Key128 cur[N];
-#pragma unroll
-  for (int j = 0; j < N; ++j) idx[j] = slot_hash(h[j], l[j]) & mask;
-#pragma unroll
-  for (int j = 0; j < N; ++j) cur[j] = ld_key(tab + idx[j]);
-#pragma unroll
-  for (int j = 0; j < N; ++j) {
-    int isnew = 0;
-    const int r = insert_min(tab, mask, idx[j], cur[j], h[j], l[j], pay_of(k, g[j]), isnew);
-    if (r > 0) {
-      atomicOr(I.bitmap + (g[j] >> 5), 1u << (g[j] & 31));
-      ++cnt.tent;
-    } else if (r < 0) {
-      ++cnt.fail;
-    }
-    cnt.fresh += isnew;
-  }
-}
-
-template <int MODE>
-__device__ void p1_unary(InstDev& I, const TileSh& P, const uint64_t* sS, int sp, P1Count& cnt) {
-  const uint64_t a = P.s0 + threadIdx.x;
-  if (a >= P.nS) return;
-  const uint64_t* srow = sS + threadIdx.x * sp;
-  KeyAcc k0, k1, k2, k3;
-  key_init(k0); key_init(k1); key_init(k2); key_init(k3);
-  for (int t = 0; t < P.T; ++t) {
-    const uint64_t w = srow[t];
-    const int L = P.len[t], off = P.off[t], wd = P.wid[t];
-    const uint64_t lm = len_mask(L);
-    key_word<MODE>(k0, ~w & lm, t, P.half, off, wd, P.stride, L);
-    key_word<MODE>(k1, w >> 1, t, P.half, off, wd, P.stride, L);
-    key_word<MODE>(k2, w_fin(w), t, P.half, off, wd, P.stride, L);
-    key_word<MODE>(k3, w_glob(w, lm), t, P.half, off, wd, P.stride, L);
-  }
-  uint64_t h[4], l[4], g[4];
-  key_final<MODE>(k0, h[0], l[0]);
-  key_final<MODE>(k1, h[1], l[1]);
-  key_final<MODE>(k2, h[2], l[2]);
-  key_final<MODE>(k3, h[3], l[3]);
-  g[0] = I.base_not + a;
-  g[1] = I.base_x + a;
-  g[2] = I.base_f + a;
-  g[3] = I.base_g + a;
-  insert_group<4>(I, I.table, I.table_mask, P.k, h, l, g, cnt);
-}
-
-template <int MODE, bool FOUR>
-__device__ void p1_binary(InstDev& I, const TileSh& P, const uint64_t* sS, int sp, const uint64_t* sQ,
-                          P1Count& cnt) {
-  const uint64_t s = P.s0 + threadIdx.x;
-  if (s >= P.nS) return;
-  const uint64_t* srow = sS + threadIdx.x * sp;
-  const int nq = (int)((P.nQ - P.q0) < (uint64_t)P.tq ? (P.nQ - P.q0) : (uint64_t)P.tq);
-  for (int q = 0; q < nq; ++q) {
-    const uint64_t* qrow = sQ + q * P.TP;
-    KeyAcc kA, kO, kU, kV;
-    key_init(kA); key_init(kO); key_init(kU); key_init(kV);
-    for (int t = 0; t < P.T; ++t) {
-      const uint64_t qw = qrow[t], sw = srow[t];
-      const uint64_t la = P.qleft ? qw : sw, lb = P.qleft ? sw : qw;
-      const int L = P.len[t], off = P.off[t], wd = P.wid[t];
-      key_word<MODE>(kA, la & lb, t, P.half, off, wd, P.stride, L);
-      key_word<MODE>(kO, la | lb, t, P.half, off, wd, P.stride, L);
-      key_word<MODE>(kU, w_until(la, lb), t, P.half, off, wd, P.stride, L);
-      if (FOUR) key_word<MODE>(kV, w_until(lb, la), t, P.half, off, wd, P.stride, L);
-    }
-    const uint64_t a = P.qleft ? P.q0 + q : s;     // index in level i
-    const uint64_t b = P.qleft ? s : P.q0 + q;     // index in level j
-    uint64_t h[4], l[4], g[4];
-    key_final<MODE>(kA, h[0], l[0]);
-    key_final<MODE>(kO, h[1], l[1]);
-    key_final<MODE>(kU, h[2], l[2]);
-    const uint64_t ab = a * P.nj + b;
-    g[0] = I.base_and[P.i] + ab;
-    g[1] = I.base_or[P.i] + ab;
-    g[2] = I.base_u[P.i] + ab;
-    if (FOUR) {
-      key_final<MODE>(kV, h[3], l[3]);
-      g[3] = I.base_u[P.j] + b * P.ni + a;
-      insert_group<4>(I, I.table, I.table_mask, P.k, h, l, g, cnt);
-    } else {
-      insert_group<3>(I, I.table, I.table_mask, P.k, h, l, g, cnt);
-    }
-  }
-}
-
-__global__ void __launch_bounds__(kTS) k_p1(BatchDev* Bp) {
+__device__ void ph_p1(const BatchDev& B) {
   extern __shared__ __align__(16) uint64_t smem[];
   __shared__ TileSh P;
   __shared__ unsigned long long s_red[3][kTS / 32];
-  const BatchDev B = *Bp;
   const unsigned long long total = B.p1_prefix[B.ninst];
   while (true) {
     if (threadIdx.x == 0) {
@@ -544,6 +232,11 @@ __global__ void __launch_bounds__(kTS) k_p1(BatchDev* Bp) {
   }
 }
 
+__global__ void __launch_bounds__(kTS) k_p1(BatchDev* Bp) {
+  const BatchDev B = *Bp;
+  ph_p1(B);
+}
+
 // ========================================================== bitmap compaction
 // phase 0: candidate bitmap (bits = candidate index) -> I.tent
 // phase 1: winner bitmap (bits = tentative index)     -> I.wins (values I.tent[bit])
@@ -551,12 +244,11 @@ __device__ __forceinline__ uint64_t phase_bits(const InstDev& I, int phase) {
   return phase ? I.n_tent : I.cands;
 }
 
-__global__ void k_chunk_count(BatchDev* Bp, int phase) {
+__device__ void ph_chunk_count(const BatchDev& B, unsigned bid, unsigned nb, int phase) {
   __shared__ unsigned long long s_w[32];
-  const BatchDev B = *Bp;
   const unsigned long long* prefix = phase ? B.chunk_prefix1 : B.chunk_prefix0;
   const unsigned long long total = prefix[B.ninst];
-  for (unsigned long long c = blockIdx.x; c < total; c += gridDim.x) {
+  for (unsigned long long c = bid; c < total; c += nb) {
     const int b = find_owner(prefix, B.ninst, c);
     const InstDev& I = B.inst[b];
     const uint64_t words = (phase_bits(I, phase) + 31) / 32;
@@ -576,14 +268,18 @@ __global__ void k_chunk_count(BatchDev* Bp, int phase) {
   }
 }
 
+__global__ void k_chunk_count(BatchDev* Bp, int phase) {
+  const BatchDev B = *Bp;
+  ph_chunk_count(B, blockIdx.x, gridDim.x, phase);
+}
+
 // One CTA per instance: scan its chunk counts, check capacities.  The last CTA
 // to finish (ticket) builds the cross-instance prefixes of the next kernels.
-__global__ void k_chunk_scan(BatchDev* Bp, int phase) {
+__device__ void ph_chunk_scan(const BatchDev& B, unsigned bid, unsigned nb, int phase) {
   __shared__ unsigned long long s_w[32];
   __shared__ int s_last;
-  const BatchDev B = *Bp;
   const unsigned long long* prefix = phase ? B.chunk_prefix1 : B.chunk_prefix0;
-  for (int b = blockIdx.x; b < B.ninst; b += gridDim.x) {
+  for (int b = bid; b < B.ninst; b += nb) {
     InstDev& I = B.inst[b];
     if (I.status != ST_RUNNING) continue;
     const unsigned long long c0 = prefix[b], nc = prefix[b + 1] - c0;
@@ -623,7 +319,7 @@ __global__ void k_chunk_scan(BatchDev* Bp, int phase) {
   __syncthreads();
   if (threadIdx.x == 0) {
     const unsigned long long t = atomicAdd(B.tickets + 1 + phase, 1ULL);
-    s_last = (t == gridDim.x - 1);
+    s_last = (t == nb - 1);
   }
   __syncthreads();
   if (s_last && threadIdx.x == 0) {
@@ -649,17 +345,21 @@ __global__ void k_chunk_scan(BatchDev* Bp, int phase) {
   }
 }
 
+__global__ void k_chunk_scan(BatchDev* Bp, int phase) {
+  const BatchDev B = *Bp;
+  ph_chunk_scan(B, blockIdx.x, gridDim.x, phase);
+}
+
 // Emit set bits of each chunk in order; always clears the chunk's words.
 // The chunk is loaded coalesced into shared memory (padded rows of 16 words),
 // then every thread scans its 16 consecutive words.
-__global__ void __launch_bounds__(kChunkThreads) k_chunk_emit(BatchDev* Bp, int phase) {
+__device__ void ph_chunk_emit(const BatchDev& B, unsigned bid, unsigned nb, int phase) {
   __shared__ unsigned long long s_w[32];
-  constexpr int kPer = kChunkWords / kChunkThreads;   // 16 words per thread
-  __shared__ uint32_t s_bits[kChunkThreads * (kPer + 1)];
-  const BatchDev B = *Bp;
+  const int kPer = kChunkWords / blockDim.x;   // consecutive words per thread
+  __shared__ uint32_t s_bits[kChunkWords + 256];
   const unsigned long long* prefix = phase ? B.chunk_prefix1 : B.chunk_prefix0;
   const unsigned long long total = prefix[B.ninst];
-  for (unsigned long long c = blockIdx.x; c < total; c += gridDim.x) {
+  for (unsigned long long c = bid; c < total; c += nb) {
     const int b = find_owner(prefix, B.ninst, c);
     InstDev& I = B.inst[b];
     const uint64_t words = (phase_bits(I, phase) + 31) / 32;
@@ -673,20 +373,29 @@ __global__ void __launch_bounds__(kChunkThreads) k_chunk_emit(BatchDev* Bp, int 
     __syncthreads();
     const uint32_t* mine = s_bits + threadIdx.x * (kPer + 1);
     unsigned long long cnt = 0;
-#pragma unroll
     for (int u = 0; u < kPer; ++u) cnt += __popc(mine[u]);
     unsigned long long tot;
     unsigned long long pos = block_excl_scan(cnt, s_w, tot) + B.chunk_base[c];
     if (I.status == ST_RUNNING && cnt) {
       uint64_t* out = phase ? I.wins : I.tent;
       const uint64_t wbeg = cbeg + (uint64_t)threadIdx.x * kPer;
+      const uint64_t* tent = I.tent;
       for (int u = 0; u < kPer; ++u) {
-        uint32_t bits = mine[u];
-        while (bits) {
-          const int p = __ffs(bits) - 1;
-          bits &= bits - 1;
-          const uint64_t idx = (wbeg + u) * 32 + p;
-          out[pos++] = phase ? I.tent[idx] : idx;
+        const uint32_t bits = mine[u];
+        if (!bits) continue;
+        const uint64_t base = (wbeg + u) * 32;
+        if (phase) {
+          // independent read-only gathers, issued before the stores
+          uint64_t v[32];
+#pragma unroll
+          for (int p = 0; p < 32; ++p) v[p] = ((bits >> p) & 1u) ? __ldcg(tent + base + p) : 0ULL;
+#pragma unroll
+          for (int p = 0; p < 32; ++p)
+            if ((bits >> p) & 1u) out[pos++] = v[p];
+        } else {
+#pragma unroll
+          for (int p = 0; p < 32; ++p)
+            if ((bits >> p) & 1u) out[pos++] = base + p;
         }
       }
     }
@@ -694,93 +403,86 @@ __global__ void __launch_bounds__(kChunkThreads) k_chunk_emit(BatchDev* Bp, int 
   }
 }
 
-// ================================================================== verify
-__global__ void k_verify(BatchDev* Bp) {
+__global__ void __launch_bounds__(kChunkThreads) k_chunk_emit(BatchDev* Bp, int phase) {
   const BatchDev B = *Bp;
+  ph_chunk_emit(B, blockIdx.x, gridDim.x, phase);
+}
+
+// ================================================================== verify
+__device__ void ph_verify(const BatchDev& B, unsigned bid, unsigned nb) {
   const unsigned long long total = B.tent_prefix[B.ninst];
-  for (unsigned long long e = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-       e += (unsigned long long)gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const unsigned long long nwarps = ((unsigned long long)nb * blockDim.x) >> 5;
+  for (unsigned long long e = ((unsigned long long)bid * blockDim.x + threadIdx.x) >> 5; e < total;
+       e += nwarps) {
     const int b = find_owner(B.tent_prefix, B.ninst, e);
     InstDev& I = B.inst[b];
     const uint64_t i = e - B.tent_prefix[b];
     const int k = I.level;
     const uint64_t g = I.tent[i];
     const Cand c = decode(I, k, g);
+    if (c.op < 0) continue;
     uint64_t h, l;
     switch (I.key_mode) {
-      case KEY_HASH: cand_key<KEY_HASH>(I, c, h, l); break;
-      case KEY_SAMPLED: cand_key<KEY_SAMPLED>(I, c, h, l); break;
-      default: cand_key<KEY_CONCAT>(I, c, h, l);
+      case KEY_HASH: warp_key<KEY_HASH>(I, c, lane, h, l); break;
+      case KEY_SAMPLED: warp_key<KEY_SAMPLED>(I, c, lane, h, l); break;
+      default: warp_key<KEY_CONCAT>(I, c, lane, h, l);
     }
-    if (find_pay(I.table, I.table_mask, h, l) == pay_of(k, g))
+    if (lane == 0 && find_pay(I.table, I.table_mask, h, l) == pay_of(k, g))
       atomicOr(I.bitmap + (i >> 5), 1u << (i & 31));
   }
 }
 
-// ================================================================ emit rows
-__global__ void k_emit_rows(BatchDev* Bp) {
+__global__ void k_verify(BatchDev* Bp) {
   const BatchDev B = *Bp;
+  ph_verify(B, blockIdx.x, gridDim.x);
+}
+
+// ================================================================ emit rows
+// Warp per winner, lane per trace word (coalesced row reads and writes).
+__device__ void ph_emit_rows(const BatchDev& B, unsigned bid, unsigned nb) {
   const unsigned long long total = B.win_prefix[B.ninst];
-  for (unsigned long long e = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-       e += (unsigned long long)gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const unsigned long long nwarps = ((unsigned long long)nb * blockDim.x) >> 5;
+  for (unsigned long long e = ((unsigned long long)bid * blockDim.x + threadIdx.x) >> 5; e < total;
+       e += nwarps) {
     const int b = find_owner(B.win_prefix, B.ninst, e);
     InstDev& I = B.inst[b];
     const uint64_t w = e - B.win_prefix[b];
     const int k = I.level;
     const uint64_t g = I.wins[w];
     const Cand c = decode(I, k, g);
+    if (c.op < 0) continue;
     const uint64_t* ra = row_ptr(I, c.la, c.a);
     const uint64_t* rb = (c.op == OP_AND || c.op == OP_OR || c.op == OP_U) ? row_ptr(I, c.lb, c.b) : ra;
     const uint64_t r = I.lstart[k] + w;
     uint64_t* dst = I.rows + r * (uint64_t)I.TP;
-    uint64_t bad = 0;
     const int T = I.T;
-    for (int t = 0; t < I.TP; t += 2) {
-      const uint64_t w0 = apply_w(c.op, ra[t], rb[t], I.len[t]);
-      const uint64_t w1 = (t + 1 < T) ? apply_w(c.op, ra[t + 1], rb[t + 1], I.len[t + 1]) : 0ULL;
-      bad |= (w0 ^ (is_pos(I, t) ? 1ULL : 0ULL)) & 1ULL;
-      if (t + 1 < T) bad |= (w1 ^ (is_pos(I, t + 1) ? 1ULL : 0ULL)) & 1ULL;
-      *reinterpret_cast<ulonglong2*>(dst + t) = make_ulonglong2(w0, w1);
+    uint64_t bad = 0;
+    for (int t = lane; t < I.TP; t += 32) {
+      uint64_t word = 0;
+      if (t < T) {
+        word = apply_w(c.op, __ldcg(ra + t), __ldcg(rb + t), I.len[t]);
+        bad |= (word ^ (is_pos(I, t) ? 1ULL : 0ULL)) & 1ULL;
+      }
+      dst[t] = word;
     }
-    I.origin[r] = g;
-    if (!bad) atomicMin(&I.best_sol, (unsigned long long)g);
+    const bool sol = !__any_sync(0xffffffffu, bad != 0);
+    if (lane == 0) {
+      I.origin[r] = g;
+      if (sol) atomicMin(&I.best_sol, (unsigned long long)g);
+    }
   }
+}
+
+__global__ void k_emit_rows(BatchDev* Bp) {
+  const BatchDev B = *Bp;
+  ph_emit_rows(B, blockIdx.x, gridDim.x);
 }
 
 // ================================================================== finish
-// RPN of the node (level lvl, candidate g) into I.rpn (postfix).
-__device__ void reconstruct(InstDev& I, int lvl, uint64_t g) {
-  struct Fr { int lvl; uint64_t g; int state; };
-  Fr st[2 * kMaxSize + 2];
-  int sp = 0, out = 0;
-  st[0] = {lvl, g, 0};
-  while (sp >= 0 && out < kMaxSize) {
-    Fr& f = st[sp];
-    if (f.lvl <= 1) {
-      I.rpn[out++] = (int16_t)f.g;
-      --sp;
-      continue;
-    }
-    const Cand c = decode(I, f.lvl, f.g);
-    if (c.op < 0) { out = 0; break; }
-    const bool bin = (c.op == OP_AND || c.op == OP_OR || c.op == OP_U);
-    if (f.state == 0) {
-      f.state = 1;
-      st[++sp] = {c.la, I.origin[I.lstart[c.la] + c.a], 0};
-    } else if (f.state == 1 && bin) {
-      f.state = 2;
-      st[++sp] = {c.lb, I.origin[I.lstart[c.lb] + c.b], 0};
-    } else {
-      I.rpn[out++] = (int16_t)(-(1 + c.op));
-      --sp;
-    }
-  }
-  I.rpn_len = out;
-}
-
-__global__ void k_finish(BatchDev* Bp) {
-  const BatchDev B = *Bp;
-  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < B.ninst; b += gridDim.x * blockDim.x) {
+__device__ void ph_finish(const BatchDev& B, unsigned bid, unsigned nb) {
+  for (int b = bid * blockDim.x + threadIdx.x; b < B.ninst; b += nb * blockDim.x) {
     InstDev& I = B.inst[b];
     if (I.status == ST_RUNNING) {
       const int k = I.level;
@@ -809,6 +511,11 @@ __global__ void k_finish(BatchDev* Bp) {
   }
 }
 
+__global__ void k_finish(BatchDev* Bp) {
+  const BatchDev B = *Bp;
+  ph_finish(B, blockIdx.x, gridDim.x);
+}
+
 __global__ void k_loop_ctl(BatchDev* Bp, cudaGraphConditionalHandle handle, unsigned int max_iter) {
   __shared__ int s_run, s_need;
   const BatchDev B = *Bp;
@@ -827,6 +534,86 @@ __global__ void k_loop_ctl(BatchDev* Bp, cudaGraphConditionalHandle handle, unsi
     const unsigned long long it = ++(*B.loop_iter);
     const bool more = s_run && !s_need && it < max_iter;
     cudaGraphSetConditional(handle, more ? 1u : 0u);
+  }
+}
+
+// ======================================================= persistent solver
+// A wait longer than this (in SM clock cycles, ~60 s) is treated as a failed
+// barrier: the waiting CTA raises ctl[2] and every CTA leaves the kernel.
+constexpr long long kBarrierCycles = 120000000000LL;
+
+__device__ bool grid_sync(unsigned int* ctl, unsigned int nb) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int* vgen = ctl + 1;
+    volatile unsigned int* verr = ctl + 2;
+    const unsigned int gen = *vgen;
+    __threadfence();
+    const unsigned int arrived = atomicAdd(ctl, 1u) + 1u;
+    if (arrived == nb) {
+      atomicExch(ctl, 0u);     // no CTA arrives again before the generation moves
+      __threadfence();
+      atomicAdd(ctl + 1, 1u);
+    } else {
+      const long long t0 = clock64();
+      while (*vgen == gen && *verr == 0) {
+        if (clock64() - t0 > kBarrierCycles) {
+          atomicExch(ctl + 2, 1u);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    s_ok = (*verr == 0);
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+__global__ void __launch_bounds__(kTS) k_solve(BatchDev* Bp, unsigned int max_steps) {
+  const BatchDev B = *Bp;
+  unsigned int* ctl = B.ctl;
+  const unsigned int bid = blockIdx.x, nb = gridDim.x;
+  __shared__ int s_more;
+  for (unsigned int it = 0; it < max_steps; ++it) {
+    ph_plan(B, bid, nb);
+    if (!grid_sync(ctl, nb)) return;
+    if (bid == 0 && threadIdx.x == 0) ph_plan_prefix(B);
+    if (!grid_sync(ctl, nb)) return;
+    ph_p1(B);
+    if (!grid_sync(ctl, nb)) return;
+    for (int phase = 0; phase < 2; ++phase) {
+      if (phase == 1) {
+        ph_verify(B, bid, nb);
+        if (!grid_sync(ctl, nb)) return;
+      }
+      ph_chunk_count(B, bid, nb, phase);
+      if (!grid_sync(ctl, nb)) return;
+      ph_chunk_scan(B, bid, nb, phase);
+      if (!grid_sync(ctl, nb)) return;
+      ph_chunk_emit(B, bid, nb, phase);
+      if (!grid_sync(ctl, nb)) return;
+    }
+    ph_emit_rows(B, bid, nb);
+    if (!grid_sync(ctl, nb)) return;
+    ph_finish(B, bid, nb);
+    if (!grid_sync(ctl, nb)) return;
+    if (bid == 0 && threadIdx.x == 0) {
+      int run = 0, need = 0;
+      for (int b = 0; b < B.ninst; ++b) {
+        const int st = B.status_out[b].x;
+        run |= (st == ST_RUNNING);
+        need |= (st == ST_NEED_MEM);
+      }
+      atomicExch(ctl + 3, (run && !need) ? 1u : 0u);
+      ++(*B.loop_iter);
+    }
+    if (!grid_sync(ctl, nb)) return;
+    if (threadIdx.x == 0) s_more = *(volatile unsigned int*)(ctl + 3);
+    __syncthreads();
+    if (!s_more) return;
   }
 }
 

@@ -25,6 +25,8 @@ struct BatchDev {
   unsigned long long* tickets;          // [4]: P1 work ticket, scan0/scan1 done counters
   int2* status_out;                     // [ninst] (status, need) mirror for the host
   unsigned long long* loop_iter;        // level steps run by the current device-side loop
+  unsigned int* ctl;                    // persistent solver: [0] barrier arrivals, [1] barrier
+                                        // generation, [2] error, [3] continue flag
 };
 
 // Level-step kernels, launched in this order for every level.
@@ -39,6 +41,12 @@ __global__ void k_finish(BatchDev* B);
 // Device-side level loop: keeps the graph's while-node running while some
 // instance is RUNNING, none waits for memory and fewer than max_iter steps ran.
 __global__ void k_loop_ctl(BatchDev* B, cudaGraphConditionalHandle handle, unsigned int max_iter);
+
+// Persistent solver: the whole level loop in one cooperative launch (all CTAs
+// co-resident), the phases above separated by a bounded grid barrier.  Runs at
+// most max_steps levels; stops early when no instance is RUNNING or one needs
+// memory.  ctl[2] != 0 afterwards means a barrier timed out.
+__global__ void k_solve(BatchDev* B, unsigned int max_steps);
 
 // Set-up and maintenance kernels.
 __global__ void k_init(BatchDev* B);

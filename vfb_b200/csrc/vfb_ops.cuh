@@ -1,0 +1,383 @@
+// vfb_ops.cuh -- device building blocks shared by the level-step kernels
+// (vfb_kernels.cu) and the persistent solver (vfb_persist.cu): hash-set
+// insert/find, candidate decoding, key computation, P1 tile processing,
+// scans, formula reconstruction.
+#pragma once
+#include "vfb_kernels.cuh"
+
+namespace vfb {
+
+// ------------------------------------------------------------------ helpers
+__device__ __forceinline__ Key128 ld_key(const Slot* s) {
+  const ulonglong2 v = __ldcg(reinterpret_cast<const ulonglong2*>(s));
+  return Key128{v.x, v.y};
+}
+
+__device__ __forceinline__ unsigned long long pay_of(int k, uint64_t g) {
+  return ((unsigned long long)k << kPayShift) | (unsigned long long)g;
+}
+
+// Lower the key's payload to pay.  Returns 1 when pay is the key's minimum
+// after the update (the candidate may own the key), 0 otherwise.  A payload
+// equal to pay means the same candidate claimed it in an earlier attempt of
+// this level, which still counts as owning.
+__device__ __forceinline__ int claim(Slot* s, unsigned long long pay) {
+  const unsigned long long cur = __ldcg(&s->pay);
+  if (cur < pay) return 0;
+  if (cur == pay) return 1;
+  const unsigned long long old = atomicMin(&s->pay, pay);
+  return old >= pay ? 1 : 0;
+}
+
+// Insert-or-find (h,l) starting at slot idx whose key half-words were already
+// loaded into cur.  Returns 1/0 as claim(), -1 when the probe limit is hit.
+__device__ inline int insert_min(Slot* tab, uint64_t mask, uint64_t idx, Key128 cur, uint64_t h, uint64_t l,
+                          unsigned long long pay, int& isnew) {
+  for (int p = 0; p < kMaxProbes; ++p) {
+    if (p > 0) cur = ld_key(tab + idx);
+    if (cur.h == h && cur.l == l) return claim(tab + idx, pay);
+    // A real key never has a half equal to ~0 (normalised away), so a ~0 half
+    // is either an empty slot or a key being published: resolve with the CAS.
+    if (cur.h == kEmpty || cur.l == kEmpty) {
+      const Key128 old = atomicCAS(reinterpret_cast<Key128*>(tab + idx), Key128{kEmpty, kEmpty},
+                                   Key128{h, l});
+      if (old.h == kEmpty && old.l == kEmpty) {
+        isnew = 1;
+        return claim(tab + idx, pay);
+      }
+      if (old.h == h && old.l == l) return claim(tab + idx, pay);
+    }
+    idx = (idx + 1) & mask;
+  }
+  return -1;
+}
+
+// Payload of (h,l), or ~0 if the key is absent.
+__device__ inline unsigned long long find_pay(const Slot* tab, uint64_t mask, uint64_t h, uint64_t l) {
+  uint64_t idx = slot_hash(h, l) & mask;
+  for (int p = 0; p < kMaxProbes; ++p) {
+    const Key128 cur = ld_key(tab + idx);
+    if (cur.h == h && cur.l == l) return __ldcg(&tab[idx].pay);
+    if (cur.h == kEmpty && cur.l == kEmpty) return ~0ULL;
+    idx = (idx + 1) & mask;
+  }
+  return ~0ULL;
+}
+
+// Largest b with prefix[b] <= x (prefix non-decreasing, prefix[0] = 0 <= x < prefix[n]).
+__device__ __forceinline__ int find_owner(const unsigned long long* prefix, int n, unsigned long long x) {
+  int lo = 0, hi = n;  // prefix[lo] <= x < prefix[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (prefix[mid] <= x) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+template <typename V>
+__device__ __forceinline__ V warp_sum(V v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-wide exclusive scan of one value per thread (blockDim multiple of 32).
+__device__ inline unsigned long long block_excl_scan(unsigned long long v, unsigned long long* s_warp,
+                                              unsigned long long& total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  unsigned long long x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_warp[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    unsigned long long w = lane < nw ? s_warp[lane] : 0ULL;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < nw) s_warp[lane] = w;
+  }
+  __syncthreads();
+  total = s_warp[nw - 1];
+  const unsigned long long before = wid > 0 ? s_warp[wid - 1] : 0ULL;
+  __syncthreads();
+  return before + x - v;
+}
+
+__device__ __forceinline__ uint64_t apply_w(int op, uint64_t l, uint64_t r, int L) {
+  switch (op) {
+    case OP_NOT: return ~l & len_mask(L);
+    case OP_AND: return l & r;
+    case OP_OR: return l | r;
+    case OP_X: return l >> 1;
+    case OP_F: return w_fin(l);
+    case OP_G: return w_glob(l, len_mask(L));
+    default: return w_until(l, r);
+  }
+}
+
+struct Cand {
+  int op, la, lb;
+  uint64_t a, b;
+};
+
+// Canonical candidate index g of level k -> operator and operands (levels and
+// indices within them).  Block order ~ & | X F G U; & and | over left sizes
+// 1..floor((k-1)/2), U over 1..k-2; left index major (ltl_nocache.cu:169-224).
+__device__ inline Cand decode(const InstDev& I, int k, uint64_t g) {
+  const uint64_t* n = I.lcount;
+  Cand c;
+  c.lb = 0;
+  c.b = 0;
+  const uint64_t un = n[k - 1];
+  if (g < un) { c.op = OP_NOT; c.la = k - 1; c.a = g; return c; }
+  g -= un;
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int i = 1; 2 * i <= k - 1; ++i) {
+      const int j = k - 1 - i;
+      const uint64_t cnt = n[i] * n[j];
+      if (g < cnt) {
+        c.op = pass ? OP_OR : OP_AND;
+        c.la = i; c.lb = j; c.a = g / n[j]; c.b = g % n[j];
+        return c;
+      }
+      g -= cnt;
+    }
+  }
+  for (int op = OP_X; op <= OP_G; ++op) {
+    if (g < un) { c.op = op; c.la = k - 1; c.a = g; return c; }
+    g -= un;
+  }
+  for (int i = 1; i <= k - 2; ++i) {
+    const int j = k - 1 - i;
+    const uint64_t cnt = n[i] * n[j];
+    if (g < cnt) {
+      c.op = OP_U; c.la = i; c.lb = j; c.a = g / n[j]; c.b = g % n[j];
+      return c;
+    }
+    g -= cnt;
+  }
+  c.op = -1;
+  c.la = 1;
+  c.a = 0;
+  return c;
+}
+
+__device__ __forceinline__ const uint64_t* row_ptr(const InstDev& I, int lvl, uint64_t idx) {
+  return I.rows + (I.lstart[lvl] + idx) * (uint64_t)I.TP;
+}
+
+template <int MODE>
+__device__ inline void cand_key(const InstDev& I, const Cand& c, uint64_t& h, uint64_t& l) {
+  const uint64_t* ra = row_ptr(I, c.la, c.a);
+  const uint64_t* rb = (c.op == OP_AND || c.op == OP_OR || c.op == OP_U) ? row_ptr(I, c.lb, c.b) : ra;
+  KeyAcc k;
+  key_init(k);
+  const int T = I.T, half = T / 2;
+  for (int t = 0; t < T; ++t) {
+    const uint64_t w = apply_w(c.op, ra[t], rb[t], I.len[t]);
+    key_word<MODE>(k, w, t, half, I.off[t], I.width[t], I.stride1, I.len[t]);
+  }
+  key_final<MODE>(k, h, l);
+}
+
+__device__ inline void row_key(const InstDev& I, const uint64_t* row, uint64_t& h, uint64_t& l) {
+  KeyAcc k;
+  key_init(k);
+  const int T = I.T, half = T / 2;
+  switch (I.key_mode) {
+    case KEY_HASH:
+      for (int t = 0; t < T; ++t) key_word<KEY_HASH>(k, row[t], t, half, 0, 0, 0, 0);
+      key_final<KEY_HASH>(k, h, l);
+      break;
+    case KEY_SAMPLED:
+      for (int t = 0; t < T; ++t)
+        key_word<KEY_SAMPLED>(k, row[t], t, half, I.off[t], I.width[t], I.stride1, I.len[t]);
+      key_final<KEY_SAMPLED>(k, h, l);
+      break;
+    default:
+      for (int t = 0; t < T; ++t)
+        key_word<KEY_CONCAT>(k, row[t], t, half, I.off[t], I.width[t], 0, I.len[t]);
+      key_final<KEY_CONCAT>(k, h, l);
+  }
+}
+
+// ======================================================================= P1
+// Shared per-tile parameters.
+struct TileSh {
+  unsigned long long tile;
+  int inst, grp, k, T, TP, half, stride, mode, skip;
+  uint64_t s0, q0, nS, nQ, ni, nj;
+  int si, qi;   // levels of the stream / staged operand
+  int qleft;    // staged operand is the left operand of & | and of U(i->j)
+  int i, j, tq;
+  uint8_t len[kMaxTraces], off[kMaxTraces], wid[kMaxTraces];
+};
+
+// Copy nrows consecutive rows (pitch TP words, 16-byte aligned) into shared
+// memory with pitch sp, as 128-bit coalesced loads.
+__device__ __forceinline__ void stage_rows(uint64_t* dst, int sp, const uint64_t* src, int nrows, int TP) {
+  const int n2 = nrows * TP / 2;
+  const ulonglong2* s2 = reinterpret_cast<const ulonglong2*>(src);
+  for (int u = threadIdx.x; u < n2; u += blockDim.x) {
+    const ulonglong2 v = __ldcg(s2 + u);
+    const int w = 2 * u, r = w / TP, c = w - r * TP;
+    dst[r * sp + c] = v.x;
+    dst[r * sp + c + 1] = v.y;
+  }
+}
+
+struct P1Count {
+  unsigned long long tent, fresh, fail;
+};
+
+template <int N>
+__device__ __forceinline__ void insert_group(InstDev& I, Slot* tab, uint64_t mask, int k, const uint64_t* h,
+                                             const uint64_t* l, const uint64_t* g, P1Count& cnt) {
+  uint64_t idx[N];
+  Key128 cur[N];
+#pragma unroll
+  for (int j = 0; j < N; ++j) idx[j] = slot_hash(h[j], l[j]) & mask;
+#pragma unroll
+  for (int j = 0; j < N; ++j) cur[j] = ld_key(tab + idx[j]);
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    int isnew = 0;
+    const int r = insert_min(tab, mask, idx[j], cur[j], h[j], l[j], pay_of(k, g[j]), isnew);
+    if (r > 0) {
+      atomicOr(I.bitmap + (g[j] >> 5), 1u << (g[j] & 31));
+      ++cnt.tent;
+    } else if (r < 0) {
+      ++cnt.fail;
+    }
+    cnt.fresh += isnew;
+  }
+}
+
+template <int MODE>
+__device__ inline void p1_unary(InstDev& I, const TileSh& P, const uint64_t* sS, int sp, P1Count& cnt) {
+  const uint64_t a = P.s0 + threadIdx.x;
+  if (a >= P.nS) return;
+  const uint64_t* srow = sS + threadIdx.x * sp;
+  KeyAcc k0, k1, k2, k3;
+  key_init(k0); key_init(k1); key_init(k2); key_init(k3);
+  for (int t = 0; t < P.T; ++t) {
+    const uint64_t w = srow[t];
+    const int L = P.len[t], off = P.off[t], wd = P.wid[t];
+    const uint64_t lm = len_mask(L);
+    key_word<MODE>(k0, ~w & lm, t, P.half, off, wd, P.stride, L);
+    key_word<MODE>(k1, w >> 1, t, P.half, off, wd, P.stride, L);
+    key_word<MODE>(k2, w_fin(w), t, P.half, off, wd, P.stride, L);
+    key_word<MODE>(k3, w_glob(w, lm), t, P.half, off, wd, P.stride, L);
+  }
+  uint64_t h[4], l[4], g[4];
+  key_final<MODE>(k0, h[0], l[0]);
+  key_final<MODE>(k1, h[1], l[1]);
+  key_final<MODE>(k2, h[2], l[2]);
+  key_final<MODE>(k3, h[3], l[3]);
+  g[0] = I.base_not + a;
+  g[1] = I.base_x + a;
+  g[2] = I.base_f + a;
+  g[3] = I.base_g + a;
+  insert_group<4>(I, I.table, I.table_mask, P.k, h, l, g, cnt);
+}
+
+template <int MODE, bool FOUR>
+__device__ inline void p1_binary(InstDev& I, const TileSh& P, const uint64_t* sS, int sp, const uint64_t* sQ,
+                          P1Count& cnt) {
+  const uint64_t s = P.s0 + threadIdx.x;
+  if (s >= P.nS) return;
+  const uint64_t* srow = sS + threadIdx.x * sp;
+  const int nq = (int)((P.nQ - P.q0) < (uint64_t)P.tq ? (P.nQ - P.q0) : (uint64_t)P.tq);
+  for (int q = 0; q < nq; ++q) {
+    const uint64_t* qrow = sQ + q * P.TP;
+    KeyAcc kA, kO, kU, kV;
+    key_init(kA); key_init(kO); key_init(kU); key_init(kV);
+    for (int t = 0; t < P.T; ++t) {
+      const uint64_t qw = qrow[t], sw = srow[t];
+      const uint64_t la = P.qleft ? qw : sw, lb = P.qleft ? sw : qw;
+      const int L = P.len[t], off = P.off[t], wd = P.wid[t];
+      key_word<MODE>(kA, la & lb, t, P.half, off, wd, P.stride, L);
+      key_word<MODE>(kO, la | lb, t, P.half, off, wd, P.stride, L);
+      key_word<MODE>(kU, w_until(la, lb), t, P.half, off, wd, P.stride, L);
+      if (FOUR) key_word<MODE>(kV, w_until(lb, la), t, P.half, off, wd, P.stride, L);
+    }
+    const uint64_t a = P.qleft ? P.q0 + q : s;     // index in level i
+    const uint64_t b = P.qleft ? s : P.q0 + q;     // index in level j
+    uint64_t h[4], l[4], g[4];
+    key_final<MODE>(kA, h[0], l[0]);
+    key_final<MODE>(kO, h[1], l[1]);
+    key_final<MODE>(kU, h[2], l[2]);
+    const uint64_t ab = a * P.nj + b;
+    g[0] = I.base_and[P.i] + ab;
+    g[1] = I.base_or[P.i] + ab;
+    g[2] = I.base_u[P.i] + ab;
+    if (FOUR) {
+      key_final<MODE>(kV, h[3], l[3]);
+      g[3] = I.base_u[P.j] + b * P.ni + a;
+      insert_group<4>(I, I.table, I.table_mask, P.k, h, l, g, cnt);
+    } else {
+      insert_group<3>(I, I.table, I.table_mask, P.k, h, l, g, cnt);
+    }
+  }
+}
+
+// Warp per candidate, lane per trace word: the two operand rows are read
+// coalesced, every lane folds its words into a partial key, and the partial
+// keys are combined with XOR shuffles (hash mode XOR-folds by definition; the
+// bit fields of the other modes are disjoint, so XOR equals OR).
+template <int MODE>
+__device__ __forceinline__ void warp_key(const InstDev& I, const Cand& c, int lane, uint64_t& h, uint64_t& l) {
+  const uint64_t* ra = row_ptr(I, c.la, c.a);
+  const uint64_t* rb = (c.op == OP_AND || c.op == OP_OR || c.op == OP_U) ? row_ptr(I, c.lb, c.b) : ra;
+  KeyAcc k;
+  key_init(k);
+  const int T = I.T, half = T / 2;
+  for (int t = lane; t < T; t += 32) {
+    const uint64_t w = apply_w(c.op, __ldcg(ra + t), __ldcg(rb + t), I.len[t]);
+    key_word<MODE>(k, w, t, half, I.off[t], I.width[t], I.stride1, I.len[t]);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    k.a0 ^= __shfl_xor_sync(0xffffffffu, k.a0, o);
+    k.a1 ^= __shfl_xor_sync(0xffffffffu, k.a1, o);
+  }
+  key_final<MODE>(k, h, l);
+}
+
+// RPN of the node (level lvl, candidate g) into I.rpn (postfix).
+__device__ inline void reconstruct(InstDev& I, int lvl, uint64_t g) {
+  struct Fr { int lvl; uint64_t g; int state; };
+  Fr st[2 * kMaxSize + 2];
+  int sp = 0, out = 0;
+  st[0] = {lvl, g, 0};
+  while (sp >= 0 && out < kMaxSize) {
+    Fr& f = st[sp];
+    if (f.lvl <= 1) {
+      I.rpn[out++] = (int16_t)f.g;
+      --sp;
+      continue;
+    }
+    const Cand c = decode(I, f.lvl, f.g);
+    if (c.op < 0) { out = 0; break; }
+    const bool bin = (c.op == OP_AND || c.op == OP_OR || c.op == OP_U);
+    if (f.state == 0) {
+      f.state = 1;
+      st[++sp] = {c.la, I.origin[I.lstart[c.la] + c.a], 0};
+    } else if (f.state == 1 && bin) {
+      f.state = 2;
+      st[++sp] = {c.lb, I.origin[I.lstart[c.lb] + c.b], 0};
+    } else {
+      I.rpn[out++] = (int16_t)(-(1 + c.op));
+      --sp;
+    }
+  }
+  I.rpn_len = out;
+}
+
+}  // namespace vfb
