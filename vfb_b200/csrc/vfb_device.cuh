@@ -36,6 +36,7 @@ enum Status : int {
 
 enum NeedBits : int {
   NEED_BITMAP = 1, NEED_TABLE = 2, NEED_TENT = 4, NEED_ROWS = 8, NEED_LIMIT = 16,
+  NEED_PROMOTE = 32,   // level too large for the cluster solver: continue on the whole GPU
 };
 
 enum KeyMode : int { KEY_CONCAT = 0, KEY_SAMPLED = 1, KEY_HASH = 3 };
@@ -83,6 +84,8 @@ struct InstDev {
   uint32_t grp_qtiles[kGroups];
   int tq;                      // staged rows per P1 tile at this level (1..kTQ)
   int pad1;
+  unsigned long long promote_above;  // candidates per level above which the instance
+                                     // leaves the cluster solver (~0: never)
   // per-level counters
   unsigned long long n_tent, n_new, n_wins, probe_fail;
   unsigned long long best_sol;  // min candidate index of a solution winner

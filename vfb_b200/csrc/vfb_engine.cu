@@ -56,6 +56,8 @@ const int kStepSeq[] = {KP_PLAN, KP_P1, KP_COUNT, KP_SCAN, KP_EMIT, KP_VERIFY, K
                         KP_ROWS, KP_FINISH};
 constexpr int kStepLen = sizeof(kStepSeq) / sizeof(int);
 constexpr unsigned kMaxLoop = 4 * kMaxSize;
+// candidates of one level above which an instance leaves the cluster solver
+constexpr unsigned long long kPromoteAbove = 1ULL << 21;
 
 struct Prof {
   uint64_t launches = 0;
@@ -75,8 +77,17 @@ struct Engine {
   int p1_grid = 0;     // P1 CTAs
   cudaError_t last_error = cudaSuccess;
   bool use_loop = true;  // device-side while-node available
-  bool use_coop = true;  // persistent cooperative solver (k_solve)
+  bool use_coop = false;  // whole-GPU persistent cooperative solver (k_solve)
   int coop_grid = 0;
+  bool use_cluster = true;  // cluster solver first, whole GPU for promoted instances
+  int cluster_size = 0, cluster_slots = 0;
+  BatchDev* d_slots = nullptr;
+  void* d_slot_mem = nullptr;
+  int* d_order = nullptr;
+  unsigned int* d_next = nullptr;
+  int slot_cap_inst = 0;        // order capacity
+  uint64_t slot_chunk_cap = 0;  // chunks per slot
+  int slots_built = -1;         // cluster_slots the slot workspace was built for
 
   // batch workspace
   int ninst_cap = 0;
@@ -123,6 +134,14 @@ struct Engine {
     d_fail = nullptr;
     if (h_ctl) cudaFreeHost(h_ctl);
     h_ctl = nullptr;
+    if (d_slots) cudaFree(d_slots);
+    if (d_slot_mem) cudaFree(d_slot_mem);
+    if (d_order) cudaFree(d_order);
+    if (d_next) cudaFree(d_next);
+    d_slots = nullptr;
+    d_slot_mem = nullptr;
+    d_order = nullptr;
+    d_next = nullptr;
     if (ev_t0) cudaEventDestroy(ev_t0);
     if (ev_t1) cudaEventDestroy(ev_t1);
     for (auto& e : ev_k)
@@ -226,8 +245,14 @@ struct Engine {
     int coop = 0;
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
     const char* sol = std::getenv("VFB_SOLVER");
-    use_coop = coop && !profile && !(sol && std::strcmp(sol, "graph") == 0) &&
-               !(env && env[0] == '1');
+    use_coop = coop && !profile && sol && std::strcmp(sol, "coop") == 0;
+    use_cluster = !profile && !(sol && (std::strcmp(sol, "graph") == 0 || std::strcmp(sol, "coop") == 0));
+    if (use_cluster) {
+      if (cudaFuncSetAttribute(k_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsmem) != cudaSuccess)
+        use_cluster = false;
+      cudaFuncSetAttribute(k_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+      cudaGetLastError();
+    }
     return VFB_OK;
   }
 
@@ -402,6 +427,123 @@ struct Engine {
     return cudaGraphLaunch(exec, stream);
   }
 
+  // ------------------------------------------------------- cluster solver
+  // Largest cluster (16, else 8) that fits the P1 tile's shared memory; the
+  // number of clusters that can be resident at once sets the slot count.
+  void pick_cluster(int p1_smem) {
+    cluster_size = 0;
+    cluster_slots = 0;
+    for (int cs : {16, 8}) {
+      cudaLaunchConfig_t cfg = {};
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = cs;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.gridDim = dim3(cs);
+      cfg.blockDim = dim3(kTS);
+      cfg.dynamicSmemBytes = (size_t)p1_smem;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      int nc = 0;
+      if (cudaOccupancyMaxActiveClusters(&nc, (const void*)k_cluster, &cfg) == cudaSuccess && nc > 0) {
+        cluster_size = cs;
+        cluster_slots = nc;
+        return;
+      }
+      cudaGetLastError();
+    }
+  }
+
+  // Per-slot private workspace (prefix arrays, tickets, chunk arrays).
+  vfb_status ensure_slots(int n, uint64_t chunks) {
+    if (cluster_slots <= 0) return VFB_DEVICE_ERROR;
+    if (n > slot_cap_inst) {
+      if (d_order) cudaFree(d_order);
+      if (cudaMalloc(&d_order, (size_t)n * sizeof(int)) != cudaSuccess) return VFB_OOM;
+      slot_cap_inst = n;
+    }
+    if (!d_next && cudaMalloc(&d_next, sizeof(unsigned int)) != cudaSuccess) return VFB_OOM;
+    const size_t per = 5 * 2 * 8 + 4 * 8 + 16 + 8 + (size_t)chunks * 12 + 64;
+    if (!d_slots || chunks > slot_chunk_cap || cluster_slots != slots_built) {
+      if (cudaStreamSynchronize(stream) != cudaSuccess) return VFB_DEVICE_ERROR;
+      if (d_slots) cudaFree(d_slots);
+      if (d_slot_mem) cudaFree(d_slot_mem);
+      d_slots = nullptr;
+      d_slot_mem = nullptr;
+      if (cudaMalloc(&d_slots, (size_t)cluster_slots * sizeof(BatchDev)) != cudaSuccess) return VFB_OOM;
+      if (cudaMalloc(&d_slot_mem, (size_t)cluster_slots * per) != cudaSuccess) return VFB_OOM;
+      std::vector<BatchDev> hs(cluster_slots);
+      for (int c = 0; c < cluster_slots; ++c) {
+        char* m = (char*)d_slot_mem + (size_t)c * per;
+        auto take = [&](size_t bytes) { char* r = m; m += (bytes + 15) & ~size_t(15); return r; };
+        BatchDev& b = hs[c];
+        b = BatchDev{};
+        b.p1_prefix = (unsigned long long*)take(16);
+        b.chunk_prefix0 = (unsigned long long*)take(16);
+        b.chunk_prefix1 = (unsigned long long*)take(16);
+        b.tent_prefix = (unsigned long long*)take(16);
+        b.win_prefix = (unsigned long long*)take(16);
+        b.tickets = (unsigned long long*)take(32);
+        b.status_out = (int2*)take(16);
+        b.loop_iter = (unsigned long long*)take(8);
+        b.chunk_cnt = (unsigned int*)take(chunks * 4);
+        b.chunk_base = (unsigned long long*)take(chunks * 8);
+        b.chunk_cap = chunks;
+        b.ninst = 1;
+      }
+      if (cudaMemcpy(d_slots, hs.data(), hs.size() * sizeof(BatchDev), cudaMemcpyHostToDevice) != cudaSuccess)
+        return VFB_DEVICE_ERROR;
+      slot_chunk_cap = chunks;
+      slots_built = cluster_slots;
+    }
+    return VFB_OK;
+  }
+
+  // Run every active instance through the cluster solver.
+  vfb_status run_clusters(std::vector<InstHost>& H, int n, int p1_smem) {
+    std::vector<int> order;
+    uint64_t chunks = 1;
+    for (int i = 0; i < n; ++i) {
+      if (!H[i].active) continue;
+      order.push_back(i);
+      chunks = std::max<uint64_t>(chunks, (H[i].d.bitmap_words + kChunkWords - 1) / kChunkWords + 1);
+    }
+    if (order.empty()) return VFB_OK;
+    vfb_status s = ensure_slots(n, chunks);
+    if (s != VFB_OK) return s;
+    if (cudaMemcpyAsync(d_order, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice, stream) !=
+            cudaSuccess ||
+        cudaMemsetAsync(d_next, 0, sizeof(unsigned int), stream) != cudaSuccess)
+      return VFB_DEVICE_ERROR;
+    c_h2d += order.size() * sizeof(int);
+    ClusterWork w{d_slots, dInst, d_order, (int)order.size(), d_next};
+    const int slots = std::min<int>(cluster_slots, (int)order.size());
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cluster_size;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(slots * cluster_size);
+    cfg.blockDim = dim3(kTS);
+    cfg.dynamicSmemBytes = (size_t)p1_smem;
+    cfg.stream = stream;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    if (cudaLaunchKernelEx(&cfg, k_cluster, w) != cudaSuccess) return VFB_DEVICE_ERROR;
+    ++c_launch;
+    // statuses of every instance after the cluster pass
+    std::vector<InstDev> recs(n);
+    if (cudaMemcpyAsync(recs.data(), dInst, (size_t)n * sizeof(InstDev), cudaMemcpyDeviceToHost, stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(stream) != cudaSuccess)
+      return VFB_DEVICE_ERROR;
+    c_d2h += (uint64_t)n * sizeof(InstDev);
+    for (int i = 0; i < n; ++i) h_status[i] = make_int2(recs[i].status, recs[i].need);
+    return VFB_OK;
+  }
+
   // ------------------------------------------------------ instance buffers
   vfb_status alloc_buffers(InstHost& H, uint64_t rows, uint64_t slots, uint64_t words, uint64_t tents) {
     InstDev& d = H.d;
@@ -454,6 +596,7 @@ struct Engine {
     const int need = d.need;
     size_t g1, g2;
     if (need & NEED_LIMIT) return VFB_LIMIT;
+    if (need & NEED_PROMOTE) d.promote_above = ~0ULL;   // continue on the whole GPU
     if (need & NEED_ROWS) {
       const uint64_t want = std::max<uint64_t>(2 * d.row_cap, d.need_amount[3] + d.need_amount[3] / 4);
       const uint64_t used = d.lstart[d.level];
@@ -664,18 +807,27 @@ struct Engine {
     int occ = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_p1, kTS, p1_smem);
     p1_grid = sms * std::max(occ, 1);
-    int occ2 = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k_solve, kTS, p1_smem);
-    coop_grid = sms * occ2;
-    if (coop_grid <= 0) use_coop = false;
+    if (use_coop) {
+      int occ2 = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k_solve, kTS, p1_smem);
+      coop_grid = sms * occ2;
+      if (coop_grid <= 0) use_coop = false;
+    }
+    bool clusters = use_cluster;
+    if (clusters) {
+      pick_cluster(p1_smem);
+      clusters = cluster_size > 0;
+    }
 
     vfb_status rc = VFB_OK;
     uint64_t chunk_need = 0;
     for (int i = 0; i < n; ++i) {
       if (H[i].fail != VFB_OK) continue;
       const InstDev& d = H[i].d;
-      const uint64_t rows = std::max<uint64_t>(4096, (uint64_t)d.A * 16);
-      const vfb_status s = alloc_buffers(H[i], rows, 1 << 14, 1 << 14, 1 << 13);
+      const uint64_t rows = std::max<uint64_t>(clusters ? (1u << 15) : 4096, (uint64_t)d.A * 16);
+      const vfb_status s = clusters ? alloc_buffers(H[i], rows, 1 << 16, 1 << 16, 1 << 16)
+                                    : alloc_buffers(H[i], rows, 1 << 14, 1 << 14, 1 << 13);
+      H[i].d.promote_above = clusters ? kPromoteAbove : ~0ULL;
       if (s != VFB_OK) { H[i].fail = s; H[i].d.status = ST_IDLE; continue; }
       H[i].active = true;
       chunk_need += (H[i].d.bitmap_words + kChunkWords - 1) / kChunkWords;
@@ -706,6 +858,10 @@ struct Engine {
     }
     int guard = 0;
     bool first = true;
+    if (rc == VFB_OK && clusters) {
+      rc = run_clusters(H, n, p1_smem);
+      first = false;
+    }
     while (rc == VFB_OK) {
       if (!first) {
         bool running = false, grew = false;

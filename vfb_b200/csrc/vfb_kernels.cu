@@ -24,6 +24,8 @@
 // The reference's thrust::remove/copy_n compaction (storeUniqueLTLs
 // LTL_BS.cu:489-530) is replaced by the bitmap compaction; its racy
 // atomicCAS winners (LTL_BS.cu:319, hash_set.cuh:232) by min-index ownership.
+#include <cooperative_groups.h>
+
 #include "vfb_ops.cuh"
 
 namespace vfb {
@@ -77,6 +79,7 @@ __device__ void ph_plan(const BatchDev& B, unsigned bid, unsigned nb) {
       const uint64_t est = g < grow ? g : grow;
       int need = 0;
       if (g >= (1ULL << kPayShift)) need |= NEED_LIMIT;
+      if (g > I.promote_above) need |= NEED_PROMOTE;
       if (words > I.bitmap_words) { need |= NEED_BITMAP; I.need_amount[0] = words; }
       if (2 * (I.keys + est) > cap) { need |= NEED_TABLE; I.need_amount[1] = 4 * (I.keys + est); }
       if (I.lstart[k] + est > I.row_cap) { need |= NEED_ROWS; I.need_amount[3] = I.lstart[k] + est; }
@@ -614,6 +617,60 @@ __global__ void __launch_bounds__(kTS) k_solve(BatchDev* Bp, unsigned int max_st
     if (threadIdx.x == 0) s_more = *(volatile unsigned int*)(ctl + 3);
     __syncthreads();
     if (!s_more) return;
+  }
+}
+
+// ========================================================= cluster solver
+// One thread-block cluster per instance in flight: the cluster's CTAs run the
+// level phases over one instance, separated by the hardware cluster barrier;
+// each cluster then pulls the next instance from the queue.  A level above
+// the instance's promote_above (or a buffer that must grow) stops the instance
+// at a level boundary with NEED_MEM; the host continues it on the whole GPU.
+__global__ void __launch_bounds__(kTS) k_cluster(ClusterWork W) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const unsigned int rank = cl.block_rank(), csize = cl.num_blocks();
+  const unsigned int slot = blockIdx.x / csize;
+  BatchDev B = W.slots[slot];
+  __shared__ int s_idx;
+  for (;;) {
+    if (rank == 0 && threadIdx.x == 0) {
+      const unsigned int q = atomicAdd(W.next, 1u);
+      s_idx = q < (unsigned int)W.n ? W.order[q] : -1;
+    }
+    cl.sync();
+    const int idx = *cl.map_shared_rank(&s_idx, 0);
+    cl.sync();   // rank 0 rewrites s_idx only after every CTA has read it
+    if (idx < 0) break;
+    B.inst = W.insts + idx;
+    B.ninst = 1;
+    for (int it = 0; it < kMaxSize + 2; ++it) {
+      const int st = *(volatile int*)&B.inst->status;
+      cl.sync();   // every CTA has read the status before a phase may change it
+      if (st != ST_RUNNING) break;
+      ph_plan(B, rank, csize);
+      cl.sync();
+      if (rank == 0 && threadIdx.x == 0) ph_plan_prefix(B);
+      cl.sync();
+      ph_p1(B);
+      cl.sync();
+      for (int phase = 0; phase < 2; ++phase) {
+        if (phase == 1) {
+          ph_verify(B, rank, csize);
+          cl.sync();
+        }
+        ph_chunk_count(B, rank, csize, phase);
+        cl.sync();
+        ph_chunk_scan(B, rank, csize, phase);
+        cl.sync();
+        ph_chunk_emit(B, rank, csize, phase);
+        cl.sync();
+      }
+      ph_emit_rows(B, rank, csize);
+      cl.sync();
+      ph_finish(B, rank, csize);
+      cl.sync();
+    }
   }
 }
 

@@ -48,6 +48,18 @@ __global__ void k_loop_ctl(BatchDev* B, cudaGraphConditionalHandle handle, unsig
 // memory.  ctl[2] != 0 afterwards means a barrier timed out.
 __global__ void k_solve(BatchDev* B, unsigned int max_steps);
 
+// Cluster solver work list: slots[c] is cluster c's private workspace (one
+// instance at a time), insts the instance records, order the queue of record
+// indices, next its head.
+struct ClusterWork {
+  BatchDev* slots;
+  InstDev* insts;
+  const int* order;
+  int n;
+  unsigned int* next;
+};
+__global__ void k_cluster(ClusterWork W);
+
 // Set-up and maintenance kernels.
 __global__ void k_init(BatchDev* B);
 __global__ void k_rehash(const Slot* old_tab, unsigned long long old_cap, Slot* new_tab,
