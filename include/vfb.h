@@ -136,6 +136,17 @@ typedef struct {
 int vfb_profile_read(void *ctx, vfb_kernel_stat *out, int cap);
 void vfb_profile_reset(void *ctx);
 
+/* Seeded synthetic instance (no counterpart in the reference, which ships no
+ * benchmark inputs): rejection-samples n_pos + n_neg traces with lengths
+ * uniform in [len_lo, len_hi] and i.i.d. Bernoulli(p) bits, labelled by a
+ * formula of planted_size drawn uniformly with the ltl_nocache numbering
+ * (ltl_nocache.cu:169-224, 248-287).  rng_state is a xoshiro256** state (4
+ * words) advanced in place.  Outputs words[i*num_vars+v], lengths[i] (positives
+ * first) and the planted formula's RPN tokens.  Returns 0, or -1 on bad sizes. */
+int vfb_synth_planted(uint64_t *rng_state, int num_vars, int planted_size, int n_pos, int n_neg,
+                      int len_lo, int len_hi, double p, int max_draws_per_trace, uint64_t *words_out,
+                      int *lengths_out, int16_t *rpn_out, int *rpn_len);
+
 /* Human-readable name of a status. */
 const char *vfb_status_str(vfb_status s);
 

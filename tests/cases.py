@@ -52,8 +52,7 @@ def planted_cases(count: int = 6, max_size_extra: int = 2):
         size = 4 + rng.below(4)
         t = 6 + rng.below(20)
         npos = t // 2
-        inst = synth.planted_instance(rng, a, size, npos, t - npos,
-                                      lambda: 4 + rng.below(29), 0.5, size + max_size_extra,
-                                      name=f"planted{s}")
+        inst = synth.planted_instance(rng, a, size, npos, t - npos, (4, 32), 0.5,
+                                      size + max_size_extra, name=f"planted{s}")
         out.append(inst)
     return out

@@ -46,8 +46,8 @@ def instances():
         a = 2 + rng.below(2)
         t = 3 + rng.below(5)
         size = 3 + rng.below(4)
-        inst = synth.planted_instance(rng, a, size, t // 2 + 1, t - t // 2,
-                                      lambda: 3 + rng.below(8), 0.5, size + 1, name=f"exact{s}")
+        inst = synth.planted_instance(rng, a, size, t // 2 + 1, t - t // 2, (3, 10), 0.5,
+                                      size + 1, name=f"exact{s}")
         if sum(inst.lengths()) <= 126:
             out.append((inst, size + 1, [3]))
     # relaxed keys (more than 126 trace bits): every rule
@@ -56,8 +56,8 @@ def instances():
         a = 2 + rng.below(3)
         t = 10 + rng.below(20)
         size = 4 + rng.below(4)
-        inst = synth.planted_instance(rng, a, size, t // 2, t - t // 2,
-                                      lambda: 8 + rng.below(24), 0.5, size + 1, name=f"relaxed{s}")
+        inst = synth.planted_instance(rng, a, size, t // 2, t - t // 2, (8, 31), 0.5,
+                                      size + 1, name=f"relaxed{s}")
         out.append((inst, size + 1, [1, 2, 3]))
     return out
 

@@ -68,7 +68,7 @@ class _JsonProblem(ctypes.Structure):
 
 EXPORTS = ["vfb_create", "vfb_destroy", "vfb_solve", "vfb_batch_solve", "vfb_status_str",
            "vfb_read_json", "vfb_json_free", "vfb_format_infix", "vfb_profile_read",
-           "vfb_profile_reset", "vfb_solve_noalloc"]
+           "vfb_profile_reset", "vfb_solve_noalloc", "vfb_synth_planted"]
 
 _lib = None
 

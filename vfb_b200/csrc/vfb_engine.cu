@@ -117,6 +117,17 @@ struct Engine {
 
   ~Engine() { release(); }
 
+  // Records (and with VFB_DEBUG=1 prints) the CUDA error behind a failure.
+  vfb_status dev_fail(int line) {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) last_error = e;
+    const char* dbg = std::getenv("VFB_DEBUG");
+    if (dbg && dbg[0] == '1')
+      std::fprintf(stderr, "vfb: device error at vfb_engine.cu:%d: %s\n", line,
+                   cudaGetErrorString(last_error));
+    return VFB_DEVICE_ERROR;
+  }
+
   void release() {
     if (stream) cudaStreamSynchronize(stream);
     if (exec) cudaGraphExecDestroy(exec);
@@ -259,7 +270,7 @@ struct Engine {
   // ------------------------------------------------------------ workspace
   vfb_status ensure_workspace(int ninst, uint64_t chunk_need) {
     if (ninst > ninst_cap || chunk_need > hB.chunk_cap) {
-      if (cudaStreamSynchronize(stream) != cudaSuccess) return VFB_DEVICE_ERROR;
+      if (cudaStreamSynchronize(stream) != cudaSuccess) return dev_fail(__LINE__);
       const int nc = std::max(ninst, ninst_cap);
       const uint64_t cc = std::max<uint64_t>(chunk_need, hB.chunk_cap);
       BatchDev nb{};
@@ -300,7 +311,7 @@ struct Engine {
     hB.inst = dInst;
     hB.ninst = ninst;
     if (cudaMemcpyAsync(dB, &hB, sizeof(BatchDev), cudaMemcpyHostToDevice, stream) != cudaSuccess)
-      return VFB_DEVICE_ERROR;
+      return dev_fail(__LINE__);
     c_h2d += sizeof(BatchDev);
     return VFB_OK;
   }
@@ -457,7 +468,7 @@ struct Engine {
 
   // Per-slot private workspace (prefix arrays, tickets, chunk arrays).
   vfb_status ensure_slots(int n, uint64_t chunks) {
-    if (cluster_slots <= 0) return VFB_DEVICE_ERROR;
+    if (cluster_slots <= 0) return dev_fail(__LINE__);
     if (n > slot_cap_inst) {
       if (d_order) cudaFree(d_order);
       if (cudaMalloc(&d_order, (size_t)n * sizeof(int)) != cudaSuccess) return VFB_OOM;
@@ -466,7 +477,7 @@ struct Engine {
     if (!d_next && cudaMalloc(&d_next, sizeof(unsigned int)) != cudaSuccess) return VFB_OOM;
     const size_t per = 5 * 2 * 8 + 4 * 8 + 16 + 8 + (size_t)chunks * 12 + 64;
     if (!d_slots || chunks > slot_chunk_cap || cluster_slots != slots_built) {
-      if (cudaStreamSynchronize(stream) != cudaSuccess) return VFB_DEVICE_ERROR;
+      if (cudaStreamSynchronize(stream) != cudaSuccess) return dev_fail(__LINE__);
       if (d_slots) cudaFree(d_slots);
       if (d_slot_mem) cudaFree(d_slot_mem);
       d_slots = nullptr;
@@ -493,7 +504,7 @@ struct Engine {
         b.ninst = 1;
       }
       if (cudaMemcpy(d_slots, hs.data(), hs.size() * sizeof(BatchDev), cudaMemcpyHostToDevice) != cudaSuccess)
-        return VFB_DEVICE_ERROR;
+        return dev_fail(__LINE__);
       slot_chunk_cap = chunks;
       slots_built = cluster_slots;
     }
@@ -515,7 +526,7 @@ struct Engine {
     if (cudaMemcpyAsync(d_order, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice, stream) !=
             cudaSuccess ||
         cudaMemsetAsync(d_next, 0, sizeof(unsigned int), stream) != cudaSuccess)
-      return VFB_DEVICE_ERROR;
+      return dev_fail(__LINE__);
     c_h2d += order.size() * sizeof(int);
     ClusterWork w{d_slots, dInst, d_order, (int)order.size(), d_next};
     const int slots = std::min<int>(cluster_slots, (int)order.size());
@@ -531,14 +542,14 @@ struct Engine {
     cfg.stream = stream;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    if (cudaLaunchKernelEx(&cfg, k_cluster, w) != cudaSuccess) return VFB_DEVICE_ERROR;
+    if (cudaLaunchKernelEx(&cfg, k_cluster, w) != cudaSuccess) return dev_fail(__LINE__);
     ++c_launch;
     // statuses of every instance after the cluster pass
     std::vector<InstDev> recs(n);
     if (cudaMemcpyAsync(recs.data(), dInst, (size_t)n * sizeof(InstDev), cudaMemcpyDeviceToHost, stream) !=
             cudaSuccess ||
         cudaStreamSynchronize(stream) != cudaSuccess)
-      return VFB_DEVICE_ERROR;
+      return dev_fail(__LINE__);
     c_d2h += (uint64_t)n * sizeof(InstDev);
     for (int i = 0; i < n; ++i) h_status[i] = make_int2(recs[i].status, recs[i].need);
     return VFB_OK;
@@ -590,9 +601,9 @@ struct Engine {
   vfb_status grow(InstHost& H, int idx) {
     InstDev& d = H.d;
     if (cudaMemcpyAsync(&d, dInst + idx, sizeof(InstDev), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
-      return VFB_DEVICE_ERROR;
+      return dev_fail(__LINE__);
     c_d2h += sizeof(InstDev);
-    if (cudaStreamSynchronize(stream) != cudaSuccess) return VFB_DEVICE_ERROR;
+    if (cudaStreamSynchronize(stream) != cudaSuccess) return dev_fail(__LINE__);
     const int need = d.need;
     size_t g1, g2;
     if (need & NEED_LIMIT) return VFB_LIMIT;
@@ -624,8 +635,8 @@ struct Engine {
       unsigned long long fails = 0;
       cudaMemcpyAsync(&fails, d_fail, sizeof(fails), cudaMemcpyDeviceToHost, stream);
       c_d2h += sizeof(fails);
-      if (cudaStreamSynchronize(stream) != cudaSuccess) return VFB_DEVICE_ERROR;
-      if (fails) return VFB_DEVICE_ERROR;
+      if (cudaStreamSynchronize(stream) != cudaSuccess) return dev_fail(__LINE__);
+      if (fails) return dev_fail(__LINE__);
       dfree(d.table);
       d.table = (Slot*)pt;
       d.table_mask = slots - 1;
@@ -653,7 +664,7 @@ struct Engine {
     d.status = ST_RUNNING;
     d.need = 0;
     if (cudaMemcpyAsync(dInst + idx, &d, sizeof(InstDev), cudaMemcpyHostToDevice, stream) != cudaSuccess)
-      return VFB_DEVICE_ERROR;
+      return dev_fail(__LINE__);
     c_h2d += sizeof(InstDev);
     return VFB_OK;
   }
@@ -739,7 +750,7 @@ struct Engine {
       }
       const size_t nb = (size_t)d.A * d.TP * 8;
       if (cudaMemcpyAsync(d.rows, dst, nb, cudaMemcpyHostToDevice, stream) != cudaSuccess)
-        return VFB_DEVICE_ERROR;
+        return dev_fail(__LINE__);
       c_h2d += nb;
       o += (size_t)d.A * d.TP;
     }
@@ -788,7 +799,7 @@ struct Engine {
   vfb_status batch(const vfb_instance* ins, int n, vfb_result* out) {
     const auto t0 = std::chrono::steady_clock::now();
     if (n <= 0) return VFB_OK;
-    if (cudaSetDevice(device) != cudaSuccess) return VFB_DEVICE_ERROR;
+    if (cudaSetDevice(device) != cudaSuccess) return dev_fail(__LINE__);
     c_h2d = c_d2h = c_launch = 0;
     cudaEventRecord(ev_t0, stream);
     std::vector<InstHost> H(n);
@@ -839,7 +850,7 @@ struct Engine {
       for (int i = 0; i < n; ++i) recs[i] = H[i].d;
       if (cudaMemcpyAsync(dInst, recs.data(), (size_t)n * sizeof(InstDev), cudaMemcpyHostToDevice, stream) !=
           cudaSuccess)
-        rc = VFB_DEVICE_ERROR;
+        rc = dev_fail(__LINE__);
       c_h2d += (uint64_t)n * sizeof(InstDev);
       // pageable source: the copy has been staged when the call returns
     }
@@ -900,10 +911,10 @@ struct Engine {
       first = false;
       cudaError_t e = run(n, p1_smem);
       if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-      if (e != cudaSuccess) { last_error = e; rc = VFB_DEVICE_ERROR; break; }
+      if (e != cudaSuccess) { last_error = e; rc = dev_fail(__LINE__); break; }
       if (use_coop) {
         c_launch += 1;
-        if (h_ctl[2] != 0) { rc = VFB_DEVICE_ERROR; break; }
+        if (h_ctl[2] != 0) { rc = dev_fail(__LINE__); break; }
       } else {
         c_launch += exec_loop ? 0 : (uint64_t)kStepLen;
       }
@@ -915,17 +926,17 @@ struct Engine {
       }
       if (profile) profile_step(n, H);
       if (verbose) report_progress(n);
-      if (++guard > 64 * kMaxSize) { rc = VFB_DEVICE_ERROR; break; }
+      if (++guard > 64 * kMaxSize) { rc = dev_fail(__LINE__); break; }
     }
     // results
     std::vector<InstDev> recs(n);
     if (cudaMemcpyAsync(recs.data(), dInst, (size_t)n * sizeof(InstDev), cudaMemcpyDeviceToHost, stream) !=
             cudaSuccess) {
-      if (rc == VFB_OK) rc = VFB_DEVICE_ERROR;
+      if (rc == VFB_OK) rc = dev_fail(__LINE__);
     }
     c_d2h += (uint64_t)n * sizeof(InstDev);
     cudaEventRecord(ev_t1, stream);
-    if (cudaStreamSynchronize(stream) != cudaSuccess && rc == VFB_OK) rc = VFB_DEVICE_ERROR;
+    if (cudaStreamSynchronize(stream) != cudaSuccess && rc == VFB_OK) rc = dev_fail(__LINE__);
     float dev_ms = 0;
     cudaEventElapsedTime(&dev_ms, ev_t0, ev_t1);
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

@@ -253,14 +253,51 @@ def _random_trace(rng: Rng, num_vars: int, length: int, p: float):
     return (length, [rng.bernoulli_word(length, p) for _ in range(num_vars)])
 
 
+def _native_planted(rng: Rng, num_vars, planted_size, n_pos, n_neg, lo, hi, p, max_draws):
+    """The same sampling in libvfb_b200 (vfb_synth.cpp); None if unavailable."""
+    try:
+        import ctypes
+        from . import load_library
+        lib = load_library()
+        fn = lib.vfb_synth_planted
+    except Exception:  # noqa: BLE001
+        return None
+    fn.restype = ctypes.c_int
+    t = n_pos + n_neg
+    st = (ctypes.c_uint64 * 4)(*rng.s)
+    words = (ctypes.c_uint64 * max(1, t * num_vars))()
+    lens = (ctypes.c_int * max(1, t))()
+    rpn = (ctypes.c_int16 * 64)()
+    rl = ctypes.c_int()
+    rc = fn(st, num_vars, planted_size, n_pos, n_neg, lo, hi, ctypes.c_double(p), max_draws,
+            words, lens, rpn, ctypes.byref(rl))
+    if rc != 0:
+        return None
+    rng.s = list(st)
+    traces = [(lens[i], [words[i * num_vars + v] for v in range(num_vars)]) for i in range(t)]
+    toks = [rpn[i] if rpn[i] >= 0 else OPS[-rpn[i] - 1] for i in range(rl.value)]
+    return toks, traces[:n_pos], traces[n_pos:]
+
+
 def planted_instance(rng: Rng, num_vars: int, planted_size: int, n_pos: int,
-                     n_neg: int, length_fn, p: float, max_size: int,
-                     max_draws_per_trace: int = 400, name: str = "") -> Instance:
+                     n_neg: int, lengths, p: float, max_size: int,
+                     max_draws_per_trace: int = 400, name: str = "",
+                     native: bool = True) -> Instance:
     """Rejection-sample traces labelled by a uniformly drawn planted formula.
 
-    A formula whose positive or negative class cannot be filled within
-    max_draws_per_trace * (n_pos + n_neg) draws is redrawn.
+    lengths: an int, or (lo, hi) for a length drawn uniformly per trace.  A
+    formula whose positive or negative class cannot be filled within
+    max_draws_per_trace * (n_pos + n_neg) draws is redrawn.  The native twin in
+    the library gives the same instance (same random stream) much faster.
     """
+    lo, hi = (lengths, lengths) if isinstance(lengths, int) else lengths
+    if native:
+        got = _native_planted(rng, num_vars, planted_size, n_pos, n_neg, lo, hi, p,
+                              max_draws_per_trace)
+        if got is not None:
+            rpn, pos, neg = got
+            return Instance(num_vars, pos, neg, max_size,
+                            [f"a{v}" for v in range(num_vars)], rpn, 3, name)
     counts = formula_counts(num_vars, planted_size)
     while True:
         rpn = number_to_rpn(rng.below(counts[planted_size][7]), planted_size, counts)
@@ -268,7 +305,8 @@ def planted_instance(rng: Rng, num_vars: int, planted_size: int, n_pos: int,
         budget = max_draws_per_trace * (n_pos + n_neg)
         while (len(pos) < n_pos or len(neg) < n_neg) and budget > 0:
             budget -= 1
-            length, words = _random_trace(rng, num_vars, length_fn(), p)
+            length = lo if lo == hi else rng.uniform_int(lo, hi)
+            length, words = _random_trace(rng, num_vars, length, p)
             holds = eval_rpn_word(rpn, words, length) & 1
             if holds and len(pos) < n_pos:
                 pos.append((length, words))
@@ -292,14 +330,14 @@ def config_small(seed: int = 0) -> Instance:
 def config_planted(seed: int = 1) -> Instance:
     """Planted single instance: 4 APs, size-9 planted formula, 20+20 traces of length 16."""
     rng = Rng(seed)
-    return planted_instance(rng, 4, 9, 20, 20, lambda: 16, 0.5, 13, name="planted")
+    return planted_instance(rng, 4, 9, 20, 20, 16, 0.5, 13, name="planted")
 
 
 def config_large(seed: int = 2, length: int = 64, planted_size: int = 13,
                  max_size: int = 17) -> Instance:
     """Planted large instance: 8 APs, 31 pos + 32 neg traces of length 64, p=0.3."""
     rng = Rng(seed)
-    return planted_instance(rng, 8, planted_size, 31, 32, lambda: length, 0.3,
+    return planted_instance(rng, 8, planted_size, 31, 32, length, 0.3,
                             max_size, name="large")
 
 
@@ -309,8 +347,7 @@ def batch_instance(rng: Rng, idx: int = 0) -> Instance:
     t = rng.uniform_int(4, 63)
     n_pos = t // 2 if rng.below(2) == 0 else (t + 1) // 2
     size = rng.uniform_int(5, 11)
-    return planted_instance(rng, a, size, n_pos, t - n_pos,
-                            lambda: rng.uniform_int(4, 64), 0.5, size + 4,
+    return planted_instance(rng, a, size, n_pos, t - n_pos, (4, 64), 0.5, size + 4,
                             name=f"batch{idx}")
 
 
