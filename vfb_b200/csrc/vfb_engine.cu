@@ -30,6 +30,7 @@ namespace vfb {
 namespace {
 
 struct InstHost {
+  uint64_t sig = 0; // instance signature (capacity hints)
   InstDev d;        // host copy of the device record
   bool active = false;
   vfb_status fail = VFB_OK;
@@ -174,12 +175,12 @@ struct Engine {
 
   // ------------------------------------------------------ device blocks
   // Returns a block of at least `bytes`; *got is its real size.  The smallest
-  // cached block that fits is reused and its full size becomes the capacity,
-  // so a repeated solve starts with the buffers its predecessor grew.
+  // cached block that fits and is at most 4x the request is reused (its full
+  // size becomes the capacity); larger cached blocks stay for larger requests.
   void* dalloc(size_t bytes, size_t* got) {
     if (bytes < 256) bytes = 256;
     auto it = free_blocks.lower_bound(bytes);
-    if (it != free_blocks.end()) {
+    if (it != free_blocks.end() && it->first <= 4 * bytes) {
       void* p = it->second;
       *got = it->first;
       free_blocks.erase(it);
@@ -475,7 +476,8 @@ struct Engine {
       slot_cap_inst = n;
     }
     if (!d_next && cudaMalloc(&d_next, sizeof(unsigned int)) != cudaSuccess) return VFB_OOM;
-    const size_t per = 5 * 2 * 8 + 4 * 8 + 16 + 8 + (size_t)chunks * 12 + 64;
+    // every slot starts on a 256-byte boundary (its arrays hold 8- and 16-byte words)
+    const size_t per = (5 * 2 * 8 + 4 * 8 + 16 + 8 + (size_t)chunks * 12 + 64 + 255) & ~size_t(255);
     if (!d_slots || chunks > slot_chunk_cap || cluster_slots != slots_built) {
       if (cudaStreamSynchronize(stream) != cudaSuccess) return dev_fail(__LINE__);
       if (d_slots) cudaFree(d_slots);
@@ -597,8 +599,29 @@ struct Engine {
     d.bitmap = nullptr;
   }
 
+  uint64_t c_grow = 0;   // buffer growths in the current call
+
+  // Final capacities of recently solved instances, keyed by a signature of the
+  // instance: a repeated instance starts with the buffers it ended with.
+  struct Caps { uint64_t rows, slots, words, tents; };
+  std::map<uint64_t, Caps> hints;
+
+  static uint64_t signature(const vfb_instance& in) {
+    uint64_t h = 0x9E3779B97F4A7C15ULL ^ ((uint64_t)in.num_vars << 32) ^ ((uint64_t)in.num_traces << 16) ^
+                 ((uint64_t)in.num_pos << 8) ^ (uint64_t)in.max_size ^ ((uint64_t)in.rlx_type << 56);
+    auto mix = [&](uint64_t x) {
+      h ^= x + 0x9E3779B97F4A7C15ULL + (h << 6) + (h >> 2);
+      h *= 0xBF58476D1CE4E5B9ULL;
+      h ^= h >> 31;
+    };
+    for (int i = 0; i < in.num_traces; ++i) mix((uint64_t)in.lengths[i]);
+    for (size_t i = 0; i < (size_t)in.num_traces * in.num_vars; ++i) mix(in.words[i]);
+    return h;
+  }
+
   // Grow whatever the device asked for; the level is then re-run.
   vfb_status grow(InstHost& H, int idx) {
+    ++c_grow;
     InstDev& d = H.d;
     if (cudaMemcpyAsync(&d, dInst + idx, sizeof(InstDev), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
       return dev_fail(__LINE__);
@@ -606,6 +629,11 @@ struct Engine {
     if (cudaStreamSynchronize(stream) != cudaSuccess) return dev_fail(__LINE__);
     const int need = d.need;
     size_t g1, g2;
+    if (std::getenv("VFB_DEBUG"))
+      std::fprintf(stderr, "vfb: instance %d level %d needs %d (rows %llu/%llu slots %llu keys %llu words %llu tent %llu)\n",
+                   idx, d.level, need, (unsigned long long)d.need_amount[3], (unsigned long long)d.row_cap,
+                   (unsigned long long)(d.table_mask + 1), (unsigned long long)d.keys,
+                   (unsigned long long)d.need_amount[0], (unsigned long long)d.need_amount[2]);
     if (need & NEED_LIMIT) return VFB_LIMIT;
     if (need & NEED_PROMOTE) d.promote_above = ~0ULL;   // continue on the whole GPU
     if (need & NEED_ROWS) {
@@ -835,9 +863,12 @@ struct Engine {
     for (int i = 0; i < n; ++i) {
       if (H[i].fail != VFB_OK) continue;
       const InstDev& d = H[i].d;
-      const uint64_t rows = std::max<uint64_t>(clusters ? (1u << 15) : 4096, (uint64_t)d.A * 16);
-      const vfb_status s = clusters ? alloc_buffers(H[i], rows, 1 << 16, 1 << 16, 1 << 16)
-                                    : alloc_buffers(H[i], rows, 1 << 14, 1 << 14, 1 << 13);
+      Caps c = clusters ? Caps{1u << 15, 1u << 16, 1u << 16, 1u << 16} : Caps{4096, 1u << 14, 1u << 14, 1u << 13};
+      c.rows = std::max<uint64_t>(c.rows, (uint64_t)d.A * 16);
+      H[i].sig = signature(ins[i]);
+      auto hit = hints.find(H[i].sig);
+      if (hit != hints.end()) c = hit->second;
+      const vfb_status s = alloc_buffers(H[i], c.rows, c.slots, c.words, c.tents);
       H[i].d.promote_above = clusters ? kPromoteAbove : ~0ULL;
       if (s != VFB_OK) { H[i].fail = s; H[i].d.status = ST_IDLE; continue; }
       H[i].active = true;
@@ -980,8 +1011,14 @@ struct Engine {
         }
       }
     }
-    for (int i = 0; i < n; ++i)
-      if (H[i].d.rows) free_buffers(H[i]);
+    for (int i = 0; i < n; ++i) {
+      if (!H[i].d.rows) continue;
+      if (recs[i].status == ST_FOUND || recs[i].status == ST_NOT_FOUND) {
+        if (hints.size() > 4096) hints.clear();
+        hints[H[i].sig] = Caps{recs[i].row_cap, recs[i].table_mask + 1, recs[i].bitmap_words, recs[i].tent_cap};
+      }
+      free_buffers(H[i]);
+    }
     return rc;
   }
 
