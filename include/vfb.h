@@ -111,7 +111,7 @@ vfb_status vfb_batch_solve(void *ctx, const vfb_instance *inst, int n, vfb_resul
  * VFB_NOALLOC_SCRATCH_BYTES that the library's module holds on every GPU that
  * loads it, until the process exits.  Buffers do not grow: the array holds a
  * hash set of 2^19 slots (kept at most half full), a bitmap of 2^25 candidates
- * per size, 2^19 tentative and winner entries, and about 36 MiB of level cache
+ * per size, 2^19 owner-list entries, and about 40 MiB of level cache
  * (for 40 traces, about 110000 characteristic sets); a search that needs more
  * stops with VFB_OOM and a message on stderr.  The first call on a device resolves the array's
  * address and should come before any stream capture.  All calls share the

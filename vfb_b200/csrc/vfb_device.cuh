@@ -35,7 +35,7 @@ enum Status : int {
 };
 
 enum NeedBits : int {
-  NEED_BITMAP = 1, NEED_TABLE = 2, NEED_TENT = 4, NEED_ROWS = 8, NEED_LIMIT = 16,
+  NEED_BITMAP = 1, NEED_TABLE = 2, NEED_LIST = 4, NEED_ROWS = 8, NEED_LIMIT = 16,
   NEED_PROMOTE = 32,   // level too large for the cluster solver: continue on the whole GPU
 };
 
@@ -63,14 +63,13 @@ struct InstDev {
   uint64_t row_cap;
   Slot* table;
   uint64_t table_mask;         // capacity - 1 (power of two)
-  uint32_t* bitmap;            // tentative-winner bits, one per candidate
+  uint32_t* bitmap;            // owner bits, one per candidate of the level being built
   uint64_t bitmap_words;
-  uint64_t* tent;              // tentative candidate indices (ascending)
-  uint64_t* wins;              // winner candidate indices (ascending)
-  uint64_t tent_cap;
+  uint64_t* wins;              // owners of new keys, ascending candidate index
+  uint64_t tent_cap;           // capacity of wins
   // ---- search state
   int status, level, need, pad0;
-  uint64_t need_amount[4];     // requested bitmap words / slots / tentatives / rows
+  uint64_t need_amount[4];     // requested bitmap words / slots / list entries / rows
   uint64_t lstart[kMaxSize + 2];
   uint64_t lcount[kMaxSize + 2];
   uint64_t lcands[kMaxSize + 2];
@@ -87,8 +86,10 @@ struct InstDev {
   unsigned long long promote_above;  // candidates per level above which the instance
                                      // leaves the cluster solver (~0: never)
   // per-level counters
-  unsigned long long n_tent, n_new, n_wins, probe_fail;
-  unsigned long long best_sol;  // min candidate index of a solution winner
+  unsigned long long n_new, n_wins, probe_fail;
+  unsigned long long best_cand;  // min candidate index whose CS satisfies the sample (P1)
+  unsigned long long best_sol;   // min candidate index of a solution owning its key
+  int sol_known, pad2;           // best_sol settled before the rows were emitted
   // ---- result
   int res_size, rpn_len;
   int16_t rpn[kMaxSize];

@@ -49,12 +49,11 @@ uint64_t pow2_at_most(uint64_t x) {
 }
 
 // Kernels of one level step, in launch order (ids index Engine::prof).
-enum KId { KP_PLAN, KP_P1, KP_COUNT, KP_SCAN, KP_EMIT, KP_VERIFY, KP_ROWS, KP_FINISH, KP_LOOP, KP_INIT, KP_REHASH,
+enum KId { KP_PLAN, KP_P1, KP_TSCAN, KP_COUNT, KP_SCAN, KP_EMIT, KP_ROWS, KP_FINISH, KP_LOOP, KP_INIT, KP_REHASH,
            KP_N };
-const char* const kNames[KP_N] = {"k_plan", "k_p1", "k_chunk_count", "k_chunk_scan", "k_chunk_emit", "k_verify",
-                                  "k_emit_rows", "k_finish", "k_loop_ctl", "k_init", "k_rehash"};
-const int kStepSeq[] = {KP_PLAN, KP_P1, KP_COUNT, KP_SCAN, KP_EMIT, KP_VERIFY, KP_COUNT, KP_SCAN, KP_EMIT,
-                        KP_ROWS, KP_FINISH};
+const char* const kNames[KP_N] = {"k_plan", "k_p1", "k_table_scan", "k_chunk_count", "k_chunk_scan",
+                                  "k_chunk_emit", "k_emit_rows", "k_finish", "k_loop_ctl", "k_init", "k_rehash"};
+const int kStepSeq[] = {KP_PLAN, KP_P1, KP_TSCAN, KP_COUNT, KP_SCAN, KP_EMIT, KP_ROWS, KP_FINISH};
 constexpr int kStepLen = sizeof(kStepSeq) / sizeof(int);
 constexpr unsigned kMaxLoop = 4 * kMaxSize;
 // candidates of one level above which an instance leaves the cluster solver
@@ -80,7 +79,7 @@ struct Engine {
   bool use_loop = true;  // device-side while-node available
   bool use_coop = false;  // whole-GPU persistent cooperative solver (k_solve)
   int coop_grid = 0;
-  bool use_cluster = true;  // cluster solver first, whole GPU for promoted instances
+  bool use_cluster = false;  // cluster solver first, whole GPU for promoted instances
   int cluster_size = 0, cluster_slots = 0;
   BatchDev* d_slots = nullptr;
   void* d_slot_mem = nullptr;
@@ -164,7 +163,7 @@ struct Engine {
 
   void free_workspace() {
     auto f = [&](void* p) { if (p) cudaFree(p); };
-    f(hB.p1_prefix); f(hB.chunk_prefix0); f(hB.chunk_prefix1); f(hB.tent_prefix); f(hB.win_prefix);
+    f(hB.p1_prefix); f(hB.chunk_prefix); f(hB.tscan_prefix); f(hB.win_prefix);
     f(hB.chunk_cnt); f(hB.chunk_base); f(hB.tickets); f(hB.status_out); f(hB.loop_iter); f(hB.ctl); f(dB);
     f(dInst);
     hB = BatchDev{};
@@ -258,7 +257,10 @@ struct Engine {
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
     const char* sol = std::getenv("VFB_SOLVER");
     use_coop = coop && !profile && sol && std::strcmp(sol, "coop") == 0;
-    use_cluster = !profile && !(sol && (std::strcmp(sol, "graph") == 0 || std::strcmp(sol, "coop") == 0));
+    // the cluster solver (one thread-block cluster per instance) is available
+    // with VFB_SOLVER=cluster; measured slower than the level-synchronous
+    // graph on single and batched solves, so it is not the default
+    use_cluster = !profile && sol && std::strcmp(sol, "cluster") == 0;
     if (use_cluster) {
       if (cudaFuncSetAttribute(k_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsmem) != cudaSuccess)
         use_cluster = false;
@@ -281,9 +283,8 @@ struct Engine {
   if (cudaMalloc(&p, (bytes)) != cudaSuccess) return VFB_OOM; \
   nb.field = reinterpret_cast<decltype(nb.field)>(p);
       WS_ALLOC(p1_prefix, pre)
-      WS_ALLOC(chunk_prefix0, pre)
-      WS_ALLOC(chunk_prefix1, pre)
-      WS_ALLOC(tent_prefix, pre)
+      WS_ALLOC(chunk_prefix, pre)
+      WS_ALLOC(tscan_prefix, pre)
       WS_ALLOC(win_prefix, pre)
       WS_ALLOC(chunk_cnt, std::max<uint64_t>(cc, 1) * sizeof(unsigned int))
       WS_ALLOC(chunk_base, std::max<uint64_t>(cc, 1) * sizeof(unsigned long long))
@@ -328,18 +329,14 @@ struct Engine {
     mark();
     k_p1<<<p1_grid, kTS, p1_smem, stream>>>(dB);
     mark();
-    for (int phase = 0; phase < 2; ++phase) {
-      if (phase == 1) {
-        k_verify<<<g, 256, 0, stream>>>(dB);
-        mark();
-      }
-      k_chunk_count<<<gc, 256, 0, stream>>>(dB, phase);
-      mark();
-      k_chunk_scan<<<std::min(ninst, g), kScanThreads, 0, stream>>>(dB, phase);
-      mark();
-      k_chunk_emit<<<gc, kChunkThreads, 0, stream>>>(dB, phase);
-      mark();
-    }
+    k_table_scan<<<g, 256, 0, stream>>>(dB);
+    mark();
+    k_chunk_count<<<gc, 256, 0, stream>>>(dB);
+    mark();
+    k_chunk_scan<<<std::min(ninst, g), kScanThreads, 0, stream>>>(dB);
+    mark();
+    k_chunk_emit<<<gc, kChunkThreads, 0, stream>>>(dB);
+    mark();
     k_emit_rows<<<g, 256, 0, stream>>>(dB);
     mark();
     k_finish<<<(ninst + 255) / 256, 256, 0, stream>>>(dB);
@@ -493,9 +490,8 @@ struct Engine {
         BatchDev& b = hs[c];
         b = BatchDev{};
         b.p1_prefix = (unsigned long long*)take(16);
-        b.chunk_prefix0 = (unsigned long long*)take(16);
-        b.chunk_prefix1 = (unsigned long long*)take(16);
-        b.tent_prefix = (unsigned long long*)take(16);
+        b.chunk_prefix = (unsigned long long*)take(16);
+        b.tscan_prefix = (unsigned long long*)take(16);
         b.win_prefix = (unsigned long long*)take(16);
         b.tickets = (unsigned long long*)take(32);
         b.status_out = (int2*)take(16);
@@ -565,10 +561,10 @@ struct Engine {
     void* po = dalloc(rows * 8, &g2);
     void* pt = dalloc(slots * sizeof(Slot), &g3);
     void* pb = dalloc(words * 4, &g4);
-    void* pe = dalloc(tents * 8, &g5);
     void* pw = dalloc(tents * 8, &g6);
-    if (!pr || !po || !pt || !pb || !pe || !pw) {
-      dfree(pr); dfree(po); dfree(pt); dfree(pb); dfree(pe); dfree(pw);
+    g5 = g6;
+    if (!pr || !po || !pt || !pb || !pw) {
+      dfree(pr); dfree(po); dfree(pt); dfree(pb); dfree(pw);
       return VFB_OOM;
     }
     d.rows = (uint64_t*)pr;
@@ -578,7 +574,6 @@ struct Engine {
     d.table_mask = pow2_at_most(g3 / sizeof(Slot)) - 1;
     d.bitmap = (uint32_t*)pb;
     d.bitmap_words = g4 / 4;
-    d.tent = (uint64_t*)pe;
     d.wins = (uint64_t*)pw;
     d.tent_cap = std::min(g5, g6) / 8;
     cudaMemsetAsync(d.table, 0xFF, (d.table_mask + 1) * sizeof(Slot), stream);
@@ -592,9 +587,8 @@ struct Engine {
     dfree(d.origin);
     dfree(d.table);
     dfree(d.bitmap);
-    dfree(d.tent);
     dfree(d.wins);
-    d.rows = d.origin = d.tent = d.wins = nullptr;
+    d.rows = d.origin = d.wins = nullptr;
     d.table = nullptr;
     d.bitmap = nullptr;
   }
@@ -678,16 +672,13 @@ struct Engine {
       d.bitmap = (uint32_t*)pb;
       d.bitmap_words = g1 / 4;
     }
-    if (need & NEED_TENT) {
+    if (need & NEED_LIST) {
       const uint64_t want = std::max<uint64_t>(2 * d.tent_cap, d.need_amount[2] + d.need_amount[2] / 4);
-      void* pe = dalloc(want * 8, &g1);
-      void* pw = pe ? dalloc(want * 8, &g2) : nullptr;
-      if (!pe || !pw) { dfree(pe); return VFB_OOM; }
-      dfree(d.tent);
+      void* pw = dalloc(want * 8, &g1);
+      if (!pw) return VFB_OOM;
       dfree(d.wins);
-      d.tent = (uint64_t*)pe;
       d.wins = (uint64_t*)pw;
-      d.tent_cap = std::min(g1, g2) / 8;
+      d.tent_cap = g1 / 8;
     }
     d.status = ST_RUNNING;
     d.need = 0;
@@ -794,13 +785,13 @@ struct Engine {
       const int j = k - 1 - i;
       operands += (double)(i == j ? n[i] : n[i] + n[j]) * T8;
     }
-    const double cands = (double)d.cands, tent = (double)d.n_tent, wins = (double)d.n_wins;
-    const double w0 = std::ceil(cands / 32.0) * 4, w1 = std::ceil(tent / 32.0) * 4;
-    prof[KP_P1].bytes += operands + 32.0 * cands + 4.0 * tent;
-    prof[KP_COUNT].bytes += w0 + w1;
-    prof[KP_EMIT].bytes += w0 + w1 + 8.0 * tent + 16.0 * wins;
-    prof[KP_VERIFY].bytes += tent * (2 * T8 + 32 + 8 + 4);
-    prof[KP_ROWS].bytes += wins * (2 * T8 + 8.0 * d.TP + 16);
+    const double cands = (double)d.cands, wins = (double)d.n_wins;
+    const double w0 = std::ceil(cands / 32.0) * 4;
+    prof[KP_P1].bytes += operands + 32.0 * cands;
+    prof[KP_TSCAN].bytes += 32.0 * (double)(d.table_mask + 1) + 4.0 * wins;
+    prof[KP_COUNT].bytes += w0;
+    prof[KP_EMIT].bytes += 2 * w0 + 8.0 * wins;
+    if (!d.sol_known) prof[KP_ROWS].bytes += wins * (2 * T8 + 8.0 * d.TP + 16);
   }
 
   void profile_step(int n, std::vector<InstHost>& H) {

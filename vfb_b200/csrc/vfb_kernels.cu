@@ -8,17 +8,19 @@
 //                 buffer checks                         (LTL_BS.cu:1226-1488)
 //   k_p1          every candidate: operator words -> 126-bit key -> insert
 //                 into the instance's hash set with atomicMin on the
-//                 candidate's canonical index; candidates that may own their
-//                 key set a bit in the tentative bitmap
+//                 candidate's canonical index; the smallest candidate index
+//                 whose CS satisfies the sample is recorded
 //                 (applyOperator LTL_BS.cu:183-238, makeRlxUnqChkCSs 30-110,
 //                  processUniqueCS 251-269)
-//   k_chunk_*     order-preserving compaction of the bitmap into the
-//                 ascending list of tentative candidates (count/scan/emit)
-//   k_verify      a tentative candidate owns its key iff the key's final
-//                 payload is its own index -> winner bitmap
-//   k_chunk_*     compaction of winners (ascending candidate index)
-//   k_emit_rows   winner rows appended to the level cache in canonical order;
-//                 solution test (insertInCache LTL_BS.cu:299-329)
+//   k_table_scan  a slot whose final payload carries level k holds a key first
+//                 seen at this level; its payload's index is the key's owner
+//                 (the minimum candidate index): set the owner's bit.  Also
+//                 settles whether the recorded solution candidate owns its key
+//   k_chunk_*     order-preserving compaction of the owner bitmap into the
+//                 ascending owner list (count per chunk / scan / emit)
+//   k_emit_rows   owners' rows appended to the level cache in canonical order,
+//                 solution test (insertInCache LTL_BS.cu:299-329); skipped
+//                 when the solution is already settled
 //   k_finish      level bookkeeping, formula reconstruction (LTL_BS.cu:561-705)
 //
 // The reference's thrust::remove/copy_n compaction (storeUniqueLTLs
@@ -34,7 +36,7 @@ namespace vfb {
 __device__ void ph_plan(const BatchDev& B, unsigned bid, unsigned nb) {
   for (int b = bid * blockDim.x + threadIdx.x; b < B.ninst; b += nb * blockDim.x) {
     InstDev& I = B.inst[b];
-    unsigned long long tiles = 0, chunks = 0;
+    unsigned long long tiles = 0, chunks = 0, tchunks = 0;
     if (I.status == ST_RUNNING) {
       const int k = I.level;
       const uint64_t* n = I.lcount;
@@ -83,19 +85,22 @@ __device__ void ph_plan(const BatchDev& B, unsigned bid, unsigned nb) {
       if (words > I.bitmap_words) { need |= NEED_BITMAP; I.need_amount[0] = words; }
       if (2 * (I.keys + est) > cap) { need |= NEED_TABLE; I.need_amount[1] = 4 * (I.keys + est); }
       if (I.lstart[k] + est > I.row_cap) { need |= NEED_ROWS; I.need_amount[3] = I.lstart[k] + est; }
-      if (est > I.tent_cap) { need |= NEED_TENT; I.need_amount[2] = est; }
+      if (est > I.tent_cap) { need |= NEED_LIST; I.need_amount[2] = est; }
       if (need) {
         I.status = ST_NEED_MEM;
         I.need = need;
       } else {
         tiles = t;
         chunks = (words + kChunkWords - 1) / kChunkWords;
-        I.n_tent = I.n_new = I.n_wins = I.probe_fail = 0;
-        I.best_sol = ~0ULL;
+        tchunks = (cap + kScanSlots - 1) / kScanSlots;
+        I.n_new = I.n_wins = I.probe_fail = 0;
+        I.best_cand = I.best_sol = ~0ULL;
+        I.sol_known = 0;
       }
     }
     B.p1_prefix[b + 1] = tiles;
-    B.chunk_prefix0[b + 1] = chunks;
+    B.chunk_prefix[b + 1] = chunks;
+    B.tscan_prefix[b + 1] = tchunks;
   }
 }
 
@@ -103,10 +108,12 @@ __device__ void ph_plan(const BatchDev& B, unsigned bid, unsigned nb) {
 // the work tickets of the step.
 __device__ void ph_plan_prefix(const BatchDev& B) {
   B.p1_prefix[0] = 0;
-  B.chunk_prefix0[0] = 0;
+  B.chunk_prefix[0] = 0;
+  B.tscan_prefix[0] = 0;
   for (int b = 0; b < B.ninst; ++b) {
     B.p1_prefix[b + 1] += B.p1_prefix[b];
-    B.chunk_prefix0[b + 1] += B.chunk_prefix0[b];
+    B.chunk_prefix[b + 1] += B.chunk_prefix[b];
+    B.tscan_prefix[b + 1] += B.tscan_prefix[b];
   }
   for (int i = 0; i < 4; ++i) B.tickets[i] = 0;
 }
@@ -144,6 +151,8 @@ __device__ void ph_p1(const BatchDev& B) {
         P.stride = I.stride1;
         P.mode = I.key_mode;
         P.tq = I.tq;
+        P.pos[0] = I.posmask[0];
+        P.pos[1] = I.posmask[1];
         // give up early once the table is known to be too small for this level
         const unsigned long long cap = I.table_mask + 1;
         P.skip = (*(volatile unsigned long long*)&I.probe_fail != 0) ||
@@ -183,7 +192,7 @@ __device__ void ph_p1(const BatchDev& B) {
     const int sp = P.TP + 1;                      // odd pitch: conflict-free row reads
     uint64_t* sS = smem;
     uint64_t* sQ = smem + kTS * sp;
-    P1Count cnt{0, 0, 0};
+    P1Count cnt{0, 0, ~0ULL};
     if (!P.skip) {
       const int ns = (int)((P.nS - P.s0) < (uint64_t)kTS ? (P.nS - P.s0) : (uint64_t)kTS);
       stage_rows(sS, sp, row_ptr(I, P.si, P.s0), ns, P.TP);
@@ -212,21 +221,29 @@ __device__ void ph_p1(const BatchDev& B) {
           else p1_binary<KEY_CONCAT, false>(I, P, sS, sp, sQ, cnt);
       }
     }
-    // per-tile counter flush: warp sums, then one atomic per counter
-    cnt.tent = warp_sum(cnt.tent);
+    // per-tile counter flush: warp reductions, then one atomic per counter
     cnt.fresh = warp_sum(cnt.fresh);
     cnt.fail = warp_sum(cnt.fail);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long y = __shfl_down_sync(0xffffffffu, cnt.sol, o);
+      cnt.sol = y < cnt.sol ? y : cnt.sol;
+    }
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (lane == 0) {
-      s_red[0][wid] = cnt.tent;
+      s_red[0][wid] = cnt.sol;
       s_red[1][wid] = cnt.fresh;
       s_red[2][wid] = cnt.fail;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-      unsigned long long a = 0, f = 0, x = 0;
-      for (int w = 0; w < kTS / 32; ++w) { a += s_red[0][w]; f += s_red[1][w]; x += s_red[2][w]; }
-      if (a) atomicAdd(&I.n_tent, a);
+      unsigned long long m = ~0ULL, f = 0, x = 0;
+      for (int w = 0; w < kTS / 32; ++w) {
+        m = s_red[0][w] < m ? s_red[0][w] : m;
+        f += s_red[1][w];
+        x += s_red[2][w];
+      }
+      if (m != ~0ULL) atomicMin(&I.best_cand, m);
       if (f) atomicAdd(&I.n_new, f);
       if (P.skip) x += 1;
       if (x) atomicAdd(&I.probe_fail, x);
@@ -240,21 +257,79 @@ __global__ void __launch_bounds__(kTS) k_p1(BatchDev* Bp) {
   ph_p1(B);
 }
 
-// ========================================================== bitmap compaction
-// phase 0: candidate bitmap (bits = candidate index) -> I.tent
-// phase 1: winner bitmap (bits = tentative index)     -> I.wins (values I.tent[bit])
-__device__ __forceinline__ uint64_t phase_bits(const InstDev& I, int phase) {
-  return phase ? I.n_tent : I.cands;
+// ============================================================== table scan
+// Owners of the keys first seen at level k: every slot whose payload carries
+// level k.  One chunk of kScanSlots slots per CTA iteration; an empty slot's
+// payload (~0) carries no level <= 32.  One warp per instance also settles
+// whether the recorded solution candidate owns its key.
+__device__ void ph_table_scan(const BatchDev& B, unsigned bid, unsigned nb) {
+  __shared__ unsigned long long s_w[32];
+  const unsigned long long total = B.tscan_prefix[B.ninst];
+  for (unsigned long long c = bid; c < total; c += nb) {
+    const int b = find_owner(B.tscan_prefix, B.ninst, c);
+    InstDev& I = B.inst[b];
+    const unsigned long long k = (unsigned long long)I.level;
+    const uint64_t s0 = (c - B.tscan_prefix[b]) * kScanSlots;
+    const uint64_t cap = I.table_mask + 1;
+    const uint64_t s1 = (s0 + kScanSlots < cap) ? s0 + kScanSlots : cap;
+    unsigned long long cnt = 0;
+    for (uint64_t sl = s0 + threadIdx.x; sl < s1; sl += blockDim.x) {
+      const unsigned long long pay = __ldcg(&I.table[sl].pay);
+      if ((pay >> kPayShift) == k) {
+        const uint64_t g = pay & kIdxMask;
+        atomicOr(I.bitmap + (g >> 5), 1u << (g & 31));
+        ++cnt;
+      }
+    }
+    cnt = warp_sum(cnt);
+    if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned long long t = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_w[w];
+      if (t) atomicAdd(&I.n_wins, t);
+    }
+    __syncthreads();
+  }
+  // solution candidate ownership (warp per instance)
+  const int lane = threadIdx.x & 31;
+  const unsigned long long gw = ((unsigned long long)bid * blockDim.x + threadIdx.x) >> 5;
+  const unsigned long long nw = ((unsigned long long)nb * blockDim.x) >> 5;
+  for (unsigned long long b = gw; b < (unsigned long long)B.ninst; b += nw) {
+    InstDev& I = B.inst[b];
+    if (I.status != ST_RUNNING || I.best_cand == ~0ULL) continue;
+    const int k = I.level;
+    const uint64_t g = I.best_cand;
+    const Cand cd = decode(I, k, g);
+    if (cd.op < 0) continue;
+    uint64_t h, l;
+    switch (I.key_mode) {
+      case KEY_HASH: warp_key<KEY_HASH>(I, cd, lane, h, l); break;
+      case KEY_SAMPLED: warp_key<KEY_SAMPLED>(I, cd, lane, h, l); break;
+      default: warp_key<KEY_CONCAT>(I, cd, lane, h, l);
+    }
+    if (lane == 0 && find_pay(I.table, I.table_mask, h, l) == pay_of(k, g)) {
+      I.best_sol = g;
+      I.sol_known = 1;
+    }
+  }
 }
 
-__device__ void ph_chunk_count(const BatchDev& B, unsigned bid, unsigned nb, int phase) {
+__global__ void k_table_scan(BatchDev* Bp) {
+  const BatchDev B = *Bp;
+  ph_table_scan(B, blockIdx.x, gridDim.x);
+}
+
+// ========================================================== bitmap compaction
+// Owner bitmap (bit g = candidate g owns a new key) -> ascending list I.wins.
+__device__ void ph_chunk_count(const BatchDev& B, unsigned bid, unsigned nb) {
   __shared__ unsigned long long s_w[32];
-  const unsigned long long* prefix = phase ? B.chunk_prefix1 : B.chunk_prefix0;
+  const unsigned long long* prefix = B.chunk_prefix;
   const unsigned long long total = prefix[B.ninst];
   for (unsigned long long c = bid; c < total; c += nb) {
     const int b = find_owner(prefix, B.ninst, c);
     const InstDev& I = B.inst[b];
-    const uint64_t words = (phase_bits(I, phase) + 31) / 32;
+    const uint64_t words = (I.cands + 31) / 32;
     const uint64_t w0 = (c - prefix[b]) * kChunkWords;
     const uint64_t w1 = (w0 + kChunkWords < words) ? w0 + kChunkWords : words;
     unsigned long long s = 0;
@@ -271,17 +346,18 @@ __device__ void ph_chunk_count(const BatchDev& B, unsigned bid, unsigned nb, int
   }
 }
 
-__global__ void k_chunk_count(BatchDev* Bp, int phase) {
+__global__ void k_chunk_count(BatchDev* Bp) {
   const BatchDev B = *Bp;
-  ph_chunk_count(B, blockIdx.x, gridDim.x, phase);
+  ph_chunk_count(B, blockIdx.x, gridDim.x);
 }
 
-// One CTA per instance: scan its chunk counts, check capacities.  The last CTA
-// to finish (ticket) builds the cross-instance prefixes of the next kernels.
-__device__ void ph_chunk_scan(const BatchDev& B, unsigned bid, unsigned nb, int phase) {
+// One CTA per instance: buffer checks for the level's new keys, scan of its
+// chunk counts.  The last CTA to finish (ticket) builds the owners' prefix
+// over instances.
+__device__ void ph_chunk_scan(const BatchDev& B, unsigned bid, unsigned nb) {
   __shared__ unsigned long long s_w[32];
   __shared__ int s_last;
-  const unsigned long long* prefix = phase ? B.chunk_prefix1 : B.chunk_prefix0;
+  const unsigned long long* prefix = B.chunk_prefix;
   for (int b = bid; b < B.ninst; b += nb) {
     InstDev& I = B.inst[b];
     if (I.status != ST_RUNNING) continue;
@@ -297,20 +373,15 @@ __device__ void ph_chunk_scan(const BatchDev& B, unsigned bid, unsigned nb, int 
     }
     if (threadIdx.x == 0) {
       int need = 0;
-      if (phase == 0) {
-        I.keys += I.n_new;
-        const unsigned long long cap = I.table_mask + 1;
-        if (I.probe_fail != 0 || 4 * I.keys > 3 * cap) {
-          need |= NEED_TABLE;
-          I.need_amount[1] = 4 * I.keys + 4096;
-        }
-        I.n_tent = running;
-        if (running > I.tent_cap) { need |= NEED_TENT; I.need_amount[2] = running; }
-      } else {
-        I.n_wins = running;
-        const uint64_t rows = I.lstart[I.level] + running;
-        if (rows > I.row_cap) { need |= NEED_ROWS; I.need_amount[3] = rows; }
+      const unsigned long long cap = I.table_mask + 1;
+      if (I.probe_fail != 0 || 4 * (I.keys + I.n_wins) > 3 * cap) {
+        need |= NEED_TABLE;
+        I.need_amount[1] = 4 * (I.keys + I.n_wins) + 4096;
       }
+      if (running > I.tent_cap) { need |= NEED_LIST; I.need_amount[2] = running; }
+      const uint64_t rows = I.lstart[I.level] + running;
+      if (!I.sol_known && rows > I.row_cap) { need |= NEED_ROWS; I.need_amount[3] = rows; }
+      I.n_wins = running;
       if (need) {
         I.status = ST_NEED_MEM;
         I.need = need;
@@ -321,51 +392,40 @@ __device__ void ph_chunk_scan(const BatchDev& B, unsigned bid, unsigned nb, int 
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
-    const unsigned long long t = atomicAdd(B.tickets + 1 + phase, 1ULL);
+    const unsigned long long t = atomicAdd(B.tickets + 1, 1ULL);
     s_last = (t == nb - 1);
   }
   __syncthreads();
   if (s_last && threadIdx.x == 0) {
     __threadfence();
-    if (phase == 0) {
-      B.tent_prefix[0] = 0;
-      B.chunk_prefix1[0] = 0;
-      for (int b = 0; b < B.ninst; ++b) {
-        const InstDev& I = B.inst[b];
-        const bool run = *(volatile const int*)&I.status == ST_RUNNING;
-        const unsigned long long nt = run ? *(volatile const unsigned long long*)&I.n_tent : 0ULL;
-        B.tent_prefix[b + 1] = B.tent_prefix[b] + nt;
-        B.chunk_prefix1[b + 1] = B.chunk_prefix1[b] + ((nt + 31) / 32 + kChunkWords - 1) / kChunkWords;
-      }
-    } else {
-      B.win_prefix[0] = 0;
-      for (int b = 0; b < B.ninst; ++b) {
-        const InstDev& I = B.inst[b];
-        const bool run = *(volatile const int*)&I.status == ST_RUNNING;
-        B.win_prefix[b + 1] = B.win_prefix[b] + (run ? *(volatile const unsigned long long*)&I.n_wins : 0ULL);
-      }
+    B.win_prefix[0] = 0;
+    for (int b = 0; b < B.ninst; ++b) {
+      const InstDev& I = B.inst[b];
+      const bool run = *(volatile const int*)&I.status == ST_RUNNING &&
+                       *(volatile const int*)&I.sol_known == 0;
+      B.win_prefix[b + 1] = B.win_prefix[b] + (run ? *(volatile const unsigned long long*)&I.n_wins : 0ULL);
     }
   }
 }
 
-__global__ void k_chunk_scan(BatchDev* Bp, int phase) {
+__global__ void k_chunk_scan(BatchDev* Bp) {
   const BatchDev B = *Bp;
-  ph_chunk_scan(B, blockIdx.x, gridDim.x, phase);
+  ph_chunk_scan(B, blockIdx.x, gridDim.x);
 }
 
 // Emit set bits of each chunk in order; always clears the chunk's words.
-// The chunk is loaded coalesced into shared memory (padded rows of 16 words),
-// then every thread scans its 16 consecutive words.
-__device__ void ph_chunk_emit(const BatchDev& B, unsigned bid, unsigned nb, int phase) {
+// The chunk is loaded coalesced into shared memory (padded rows), then every
+// thread scans its consecutive words.
+__device__ void ph_chunk_emit(const BatchDev& B, unsigned bid, unsigned nb) {
   __shared__ unsigned long long s_w[32];
   const int kPer = kChunkWords / blockDim.x;   // consecutive words per thread
   __shared__ uint32_t s_bits[kChunkWords + 256];
-  const unsigned long long* prefix = phase ? B.chunk_prefix1 : B.chunk_prefix0;
+  const unsigned long long* prefix = B.chunk_prefix;
   const unsigned long long total = prefix[B.ninst];
   for (unsigned long long c = bid; c < total; c += nb) {
     const int b = find_owner(prefix, B.ninst, c);
     InstDev& I = B.inst[b];
-    const uint64_t words = (phase_bits(I, phase) + 31) / 32;
+    const uint64_t words = (I.cands + 31) / 32;
     const uint64_t cbeg = (c - prefix[b]) * kChunkWords;
     for (int u = threadIdx.x; u < kChunkWords; u += blockDim.x) {
       const uint64_t w = cbeg + u;
@@ -380,65 +440,24 @@ __device__ void ph_chunk_emit(const BatchDev& B, unsigned bid, unsigned nb, int 
     unsigned long long tot;
     unsigned long long pos = block_excl_scan(cnt, s_w, tot) + B.chunk_base[c];
     if (I.status == ST_RUNNING && cnt) {
-      uint64_t* out = phase ? I.wins : I.tent;
+      uint64_t* out = I.wins;
       const uint64_t wbeg = cbeg + (uint64_t)threadIdx.x * kPer;
-      const uint64_t* tent = I.tent;
       for (int u = 0; u < kPer; ++u) {
         const uint32_t bits = mine[u];
         if (!bits) continue;
         const uint64_t base = (wbeg + u) * 32;
-        if (phase) {
-          // independent read-only gathers, issued before the stores
-          uint64_t v[32];
 #pragma unroll
-          for (int p = 0; p < 32; ++p) v[p] = ((bits >> p) & 1u) ? __ldcg(tent + base + p) : 0ULL;
-#pragma unroll
-          for (int p = 0; p < 32; ++p)
-            if ((bits >> p) & 1u) out[pos++] = v[p];
-        } else {
-#pragma unroll
-          for (int p = 0; p < 32; ++p)
-            if ((bits >> p) & 1u) out[pos++] = base + p;
-        }
+        for (int p = 0; p < 32; ++p)
+          if ((bits >> p) & 1u) out[pos++] = base + p;
       }
     }
     __syncthreads();
   }
 }
 
-__global__ void __launch_bounds__(kChunkThreads) k_chunk_emit(BatchDev* Bp, int phase) {
+__global__ void __launch_bounds__(kChunkThreads) k_chunk_emit(BatchDev* Bp) {
   const BatchDev B = *Bp;
-  ph_chunk_emit(B, blockIdx.x, gridDim.x, phase);
-}
-
-// ================================================================== verify
-__device__ void ph_verify(const BatchDev& B, unsigned bid, unsigned nb) {
-  const unsigned long long total = B.tent_prefix[B.ninst];
-  const int lane = threadIdx.x & 31;
-  const unsigned long long nwarps = ((unsigned long long)nb * blockDim.x) >> 5;
-  for (unsigned long long e = ((unsigned long long)bid * blockDim.x + threadIdx.x) >> 5; e < total;
-       e += nwarps) {
-    const int b = find_owner(B.tent_prefix, B.ninst, e);
-    InstDev& I = B.inst[b];
-    const uint64_t i = e - B.tent_prefix[b];
-    const int k = I.level;
-    const uint64_t g = I.tent[i];
-    const Cand c = decode(I, k, g);
-    if (c.op < 0) continue;
-    uint64_t h, l;
-    switch (I.key_mode) {
-      case KEY_HASH: warp_key<KEY_HASH>(I, c, lane, h, l); break;
-      case KEY_SAMPLED: warp_key<KEY_SAMPLED>(I, c, lane, h, l); break;
-      default: warp_key<KEY_CONCAT>(I, c, lane, h, l);
-    }
-    if (lane == 0 && find_pay(I.table, I.table_mask, h, l) == pay_of(k, g))
-      atomicOr(I.bitmap + (i >> 5), 1u << (i & 31));
-  }
-}
-
-__global__ void k_verify(BatchDev* Bp) {
-  const BatchDev B = *Bp;
-  ph_verify(B, blockIdx.x, gridDim.x);
+  ph_chunk_emit(B, blockIdx.x, gridDim.x);
 }
 
 // ================================================================ emit rows
@@ -455,7 +474,7 @@ __device__ void ph_emit_rows(const BatchDev& B, unsigned bid, unsigned nb) {
     const int k = I.level;
     const uint64_t g = I.wins[w];
     const Cand c = decode(I, k, g);
-    if (c.op < 0) continue;
+    if (c.op < 0) continue;   // (instances whose solution is settled have no winners listed)
     const uint64_t* ra = row_ptr(I, c.la, c.a);
     const uint64_t* rb = (c.op == OP_AND || c.op == OP_OR || c.op == OP_U) ? row_ptr(I, c.lb, c.b) : ra;
     const uint64_t r = I.lstart[k] + w;
@@ -489,6 +508,7 @@ __device__ void ph_finish(const BatchDev& B, unsigned bid, unsigned nb) {
     InstDev& I = B.inst[b];
     if (I.status == ST_RUNNING) {
       const int k = I.level;
+      I.keys += I.n_wins;
       if (I.best_sol != ~0ULL) {
         const uint64_t g = I.best_sol;
         uint64_t lo = 0, hi = I.n_wins;   // first index with wins[idx] >= g
@@ -587,18 +607,14 @@ __global__ void __launch_bounds__(kTS) k_solve(BatchDev* Bp, unsigned int max_st
     if (!grid_sync(ctl, nb)) return;
     ph_p1(B);
     if (!grid_sync(ctl, nb)) return;
-    for (int phase = 0; phase < 2; ++phase) {
-      if (phase == 1) {
-        ph_verify(B, bid, nb);
-        if (!grid_sync(ctl, nb)) return;
-      }
-      ph_chunk_count(B, bid, nb, phase);
-      if (!grid_sync(ctl, nb)) return;
-      ph_chunk_scan(B, bid, nb, phase);
-      if (!grid_sync(ctl, nb)) return;
-      ph_chunk_emit(B, bid, nb, phase);
-      if (!grid_sync(ctl, nb)) return;
-    }
+    ph_table_scan(B, bid, nb);
+    if (!grid_sync(ctl, nb)) return;
+    ph_chunk_count(B, bid, nb);
+    if (!grid_sync(ctl, nb)) return;
+    ph_chunk_scan(B, bid, nb);
+    if (!grid_sync(ctl, nb)) return;
+    ph_chunk_emit(B, bid, nb);
+    if (!grid_sync(ctl, nb)) return;
     ph_emit_rows(B, bid, nb);
     if (!grid_sync(ctl, nb)) return;
     ph_finish(B, bid, nb);
@@ -654,18 +670,14 @@ __global__ void __launch_bounds__(kTS) k_cluster(ClusterWork W) {
       cl.sync();
       ph_p1(B);
       cl.sync();
-      for (int phase = 0; phase < 2; ++phase) {
-        if (phase == 1) {
-          ph_verify(B, rank, csize);
-          cl.sync();
-        }
-        ph_chunk_count(B, rank, csize, phase);
-        cl.sync();
-        ph_chunk_scan(B, rank, csize, phase);
-        cl.sync();
-        ph_chunk_emit(B, rank, csize, phase);
-        cl.sync();
-      }
+      ph_table_scan(B, rank, csize);
+      cl.sync();
+      ph_chunk_count(B, rank, csize);
+      cl.sync();
+      ph_chunk_scan(B, rank, csize);
+      cl.sync();
+      ph_chunk_emit(B, rank, csize);
+      cl.sync();
       ph_emit_rows(B, rank, csize);
       cl.sync();
       ph_finish(B, rank, csize);

@@ -5,8 +5,9 @@
 namespace vfb {
 
 constexpr int kChunkWords = 4096;     // bitmap words per compaction chunk (131072 bits)
-constexpr int kChunkThreads = 256;    // threads per compaction CTA (16 words each)
+constexpr int kChunkThreads = 256;    // threads per compaction CTA
 constexpr int kScanThreads = 1024;
+constexpr int kScanSlots = 8192;      // hash-set slots per table-scan chunk
 
 // Global batch descriptor, resident in device memory so that buffer growth
 // never invalidates a captured launch sequence.
@@ -15,14 +16,13 @@ struct BatchDev {
   int ninst;
   int pad;
   unsigned long long* p1_prefix;        // [ninst+1] P1 tiles
-  unsigned long long* chunk_prefix0;    // [ninst+1] candidate-bitmap chunks
-  unsigned long long* chunk_prefix1;    // [ninst+1] winner-bitmap chunks
-  unsigned long long* tent_prefix;      // [ninst+1]
-  unsigned long long* win_prefix;       // [ninst+1]
+  unsigned long long* chunk_prefix;     // [ninst+1] owner-bitmap chunks
+  unsigned long long* tscan_prefix;     // [ninst+1] table-scan chunks
+  unsigned long long* win_prefix;       // [ninst+1] owners of new keys
   unsigned int* chunk_cnt;              // [chunk_cap]
   unsigned long long* chunk_base;       // [chunk_cap]
   unsigned long long chunk_cap;
-  unsigned long long* tickets;          // [4]: P1 work ticket, scan0/scan1 done counters
+  unsigned long long* tickets;          // [4]: P1 work ticket, scan done counter
   int2* status_out;                     // [ninst] (status, need) mirror for the host
   unsigned long long* loop_iter;        // level steps run by the current device-side loop
   unsigned int* ctl;                    // persistent solver: [0] barrier arrivals, [1] barrier
@@ -32,10 +32,10 @@ struct BatchDev {
 // Level-step kernels, launched in this order for every level.
 __global__ void k_plan(BatchDev* B);
 __global__ void k_p1(BatchDev* B);
-__global__ void k_chunk_count(BatchDev* B, int phase);
-__global__ void k_chunk_scan(BatchDev* B, int phase);
-__global__ void k_chunk_emit(BatchDev* B, int phase);
-__global__ void k_verify(BatchDev* B);
+__global__ void k_table_scan(BatchDev* B);
+__global__ void k_chunk_count(BatchDev* B);
+__global__ void k_chunk_scan(BatchDev* B);
+__global__ void k_chunk_emit(BatchDev* B);
 __global__ void k_emit_rows(BatchDev* B);
 __global__ void k_finish(BatchDev* B);
 // Device-side level loop: keeps the graph's while-node running while some

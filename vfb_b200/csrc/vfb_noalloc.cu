@@ -11,7 +11,7 @@
 //
 // This entry point runs the same level-step kernels as vfb_solve, but every
 // device buffer they use -- the per-instance record, the level cache, the
-// hash set, the candidate bitmap, the tentative/winner lists and the batch
+// hash set, the owner bitmap, the owner list and the batch
 // workspace -- is carved out of one file-scope static device array of
 // kScratchBytes.  Buffers never grow: a search that needs more room than the
 // array provides stops with VFB_OOM and a message on stderr.  Nothing is
@@ -40,7 +40,7 @@ namespace {
 constexpr size_t kScratchBytes = 64ull << 20;   // VFB_NOALLOC_SCRATCH_BYTES in vfb.h
 constexpr uint64_t kNaSlots = 1ull << 19;        // hash-set slots (16 MiB)
 constexpr uint64_t kNaWords = 1ull << 20;        // candidate-bitmap words (32 Mi candidates)
-constexpr uint64_t kNaTents = 1ull << 19;        // tentative / winner entries each
+constexpr uint64_t kNaTents = 1ull << 19;        // owner-list entries
 
 __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
@@ -144,7 +144,7 @@ const char* need_text(int need) {
   if (need & NEED_ROWS) return "level cache";
   if (need & NEED_TABLE) return "hash set";
   if (need & NEED_BITMAP) return "candidate bitmap";
-  if (need & NEED_TENT) return "tentative list";
+  if (need & NEED_LIST) return "owner list";
   return "index range";
 }
 
@@ -173,9 +173,8 @@ extern "C" vfb_status vfb_solve_noalloc(const vfb_instance* inst, vfb_result* ou
   hB.inst = dI;
   hB.ninst = 1;
   hB.p1_prefix = cv.take<unsigned long long>(2);
-  hB.chunk_prefix0 = cv.take<unsigned long long>(2);
-  hB.chunk_prefix1 = cv.take<unsigned long long>(2);
-  hB.tent_prefix = cv.take<unsigned long long>(2);
+  hB.chunk_prefix = cv.take<unsigned long long>(2);
+  hB.tscan_prefix = cv.take<unsigned long long>(2);
   hB.win_prefix = cv.take<unsigned long long>(2);
   hB.tickets = cv.take<unsigned long long>(4);
   hB.status_out = cv.take<int2>(1);
@@ -187,7 +186,6 @@ extern "C" vfb_status vfb_solve_noalloc(const vfb_instance* inst, vfb_result* ou
   d.table_mask = kNaSlots - 1;
   d.bitmap = cv.take<uint32_t>(kNaWords);
   d.bitmap_words = kNaWords;
-  d.tent = cv.take<uint64_t>(kNaTents);
   d.wins = cv.take<uint64_t>(kNaTents);
   d.tent_cap = kNaTents;
   const size_t used = ((cv.off + 255) & ~size_t(255)) + 512;   // + alignment of the last two carves
@@ -236,15 +234,13 @@ extern "C" vfb_status vfb_solve_noalloc(const vfb_instance* inst, vfb_result* ou
     if (status.x != ST_RUNNING) break;
     k_plan<<<1, 1024, 0, st>>>(dB);
     k_p1<<<p1_grid, kTS, p1_smem, st>>>(dB);
-    for (int phase = 0; phase < 2; ++phase) {
-      if (phase == 1) k_verify<<<g, 256, 0, st>>>(dB);
-      k_chunk_count<<<gc, 256, 0, st>>>(dB, phase);
-      k_chunk_scan<<<1, kScanThreads, 0, st>>>(dB, phase);
-      k_chunk_emit<<<gc, kChunkThreads, 0, st>>>(dB, phase);
-    }
+    k_table_scan<<<g, 256, 0, st>>>(dB);
+    k_chunk_count<<<gc, 256, 0, st>>>(dB);
+    k_chunk_scan<<<1, kScanThreads, 0, st>>>(dB);
+    k_chunk_emit<<<gc, kChunkThreads, 0, st>>>(dB);
     k_emit_rows<<<g, 256, 0, st>>>(dB);
     k_finish<<<1, 256, 0, st>>>(dB);
-    launches += 11;
+    launches += 8;
     if (cudaGetLastError() != cudaSuccess) return out->status = VFB_DEVICE_ERROR;
   }
   InstDev r;

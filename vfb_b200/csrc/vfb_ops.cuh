@@ -216,6 +216,7 @@ struct TileSh {
   int si, qi;   // levels of the stream / staged operand
   int qleft;    // staged operand is the left operand of & | and of U(i->j)
   int i, j, tq;
+  uint64_t pos[2];   // bit t: trace t is positive
   uint8_t len[kMaxTraces], off[kMaxTraces], wid[kMaxTraces];
 };
 
@@ -233,12 +234,16 @@ __device__ __forceinline__ void stage_rows(uint64_t* dst, int sp, const uint64_t
 }
 
 struct P1Count {
-  unsigned long long tent, fresh, fail;
+  unsigned long long fresh, fail, sol;   // keys inserted, probe failures, min solution candidate
 };
 
+// Insert N keys of one thread: all home-slot loads are issued first, then the
+// keys are resolved one by one.  bad[j] == 0 marks a candidate whose step-0
+// bits match every trace's label (a solution candidate).
 template <int N>
-__device__ __forceinline__ void insert_group(InstDev& I, Slot* tab, uint64_t mask, int k, const uint64_t* h,
-                                             const uint64_t* l, const uint64_t* g, P1Count& cnt) {
+__device__ __forceinline__ void insert_group(Slot* tab, uint64_t mask, int k, const uint64_t* h,
+                                             const uint64_t* l, const uint64_t* g, const uint64_t* bad,
+                                             P1Count& cnt) {
   uint64_t idx[N];
   Key128 cur[N];
 #pragma unroll
@@ -249,14 +254,14 @@ __device__ __forceinline__ void insert_group(InstDev& I, Slot* tab, uint64_t mas
   for (int j = 0; j < N; ++j) {
     int isnew = 0;
     const int r = insert_min(tab, mask, idx[j], cur[j], h[j], l[j], pay_of(k, g[j]), isnew);
-    if (r > 0) {
-      atomicOr(I.bitmap + (g[j] >> 5), 1u << (g[j] & 31));
-      ++cnt.tent;
-    } else if (r < 0) {
-      ++cnt.fail;
-    }
+    if (r < 0) ++cnt.fail;
     cnt.fresh += isnew;
+    if (!bad[j] && g[j] < cnt.sol) cnt.sol = g[j];
   }
+}
+
+__device__ __forceinline__ uint64_t pos_bit(const TileSh& P, int t) {
+  return (P.pos[t >> 6] >> (t & 63)) & 1ULL;
 }
 
 template <int MODE>
@@ -266,14 +271,20 @@ __device__ inline void p1_unary(InstDev& I, const TileSh& P, const uint64_t* sS,
   const uint64_t* srow = sS + threadIdx.x * sp;
   KeyAcc k0, k1, k2, k3;
   key_init(k0); key_init(k1); key_init(k2); key_init(k3);
+  uint64_t bad[4] = {0, 0, 0, 0};
   for (int t = 0; t < P.T; ++t) {
     const uint64_t w = srow[t];
     const int L = P.len[t], off = P.off[t], wd = P.wid[t];
-    const uint64_t lm = len_mask(L);
-    key_word<MODE>(k0, ~w & lm, t, P.half, off, wd, P.stride, L);
-    key_word<MODE>(k1, w >> 1, t, P.half, off, wd, P.stride, L);
-    key_word<MODE>(k2, w_fin(w), t, P.half, off, wd, P.stride, L);
-    key_word<MODE>(k3, w_glob(w, lm), t, P.half, off, wd, P.stride, L);
+    const uint64_t lm = len_mask(L), pb = pos_bit(P, t);
+    const uint64_t w0 = ~w & lm, w1 = w >> 1, w2 = w_fin(w), w3 = w_glob(w, lm);
+    bad[0] |= w0 ^ pb;
+    bad[1] |= w1 ^ pb;
+    bad[2] |= w2 ^ pb;
+    bad[3] |= w3 ^ pb;
+    key_word<MODE>(k0, w0, t, P.half, off, wd, P.stride, L);
+    key_word<MODE>(k1, w1, t, P.half, off, wd, P.stride, L);
+    key_word<MODE>(k2, w2, t, P.half, off, wd, P.stride, L);
+    key_word<MODE>(k3, w3, t, P.half, off, wd, P.stride, L);
   }
   uint64_t h[4], l[4], g[4];
   key_final<MODE>(k0, h[0], l[0]);
@@ -284,7 +295,9 @@ __device__ inline void p1_unary(InstDev& I, const TileSh& P, const uint64_t* sS,
   g[1] = I.base_x + a;
   g[2] = I.base_f + a;
   g[3] = I.base_g + a;
-  insert_group<4>(I, I.table, I.table_mask, P.k, h, l, g, cnt);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) bad[j] &= 1ULL;
+  insert_group<4>(I.table, I.table_mask, P.k, h, l, g, bad, cnt);
 }
 
 template <int MODE, bool FOUR>
@@ -298,14 +311,24 @@ __device__ inline void p1_binary(InstDev& I, const TileSh& P, const uint64_t* sS
     const uint64_t* qrow = sQ + q * P.TP;
     KeyAcc kA, kO, kU, kV;
     key_init(kA); key_init(kO); key_init(kU); key_init(kV);
+    uint64_t bad[4] = {0, 0, 0, 0};
     for (int t = 0; t < P.T; ++t) {
       const uint64_t qw = qrow[t], sw = srow[t];
       const uint64_t la = P.qleft ? qw : sw, lb = P.qleft ? sw : qw;
       const int L = P.len[t], off = P.off[t], wd = P.wid[t];
-      key_word<MODE>(kA, la & lb, t, P.half, off, wd, P.stride, L);
-      key_word<MODE>(kO, la | lb, t, P.half, off, wd, P.stride, L);
-      key_word<MODE>(kU, w_until(la, lb), t, P.half, off, wd, P.stride, L);
-      if (FOUR) key_word<MODE>(kV, w_until(lb, la), t, P.half, off, wd, P.stride, L);
+      const uint64_t pb = pos_bit(P, t);
+      const uint64_t wa = la & lb, wo = la | lb, wu = w_until(la, lb);
+      bad[0] |= wa ^ pb;
+      bad[1] |= wo ^ pb;
+      bad[2] |= wu ^ pb;
+      key_word<MODE>(kA, wa, t, P.half, off, wd, P.stride, L);
+      key_word<MODE>(kO, wo, t, P.half, off, wd, P.stride, L);
+      key_word<MODE>(kU, wu, t, P.half, off, wd, P.stride, L);
+      if (FOUR) {
+        const uint64_t wv = w_until(lb, la);
+        bad[3] |= wv ^ pb;
+        key_word<MODE>(kV, wv, t, P.half, off, wd, P.stride, L);
+      }
     }
     const uint64_t a = P.qleft ? P.q0 + q : s;     // index in level i
     const uint64_t b = P.qleft ? s : P.q0 + q;     // index in level j
@@ -317,12 +340,14 @@ __device__ inline void p1_binary(InstDev& I, const TileSh& P, const uint64_t* sS
     g[0] = I.base_and[P.i] + ab;
     g[1] = I.base_or[P.i] + ab;
     g[2] = I.base_u[P.i] + ab;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) bad[j] &= 1ULL;
     if (FOUR) {
       key_final<MODE>(kV, h[3], l[3]);
       g[3] = I.base_u[P.j] + b * P.ni + a;
-      insert_group<4>(I, I.table, I.table_mask, P.k, h, l, g, cnt);
+      insert_group<4>(I.table, I.table_mask, P.k, h, l, g, bad, cnt);
     } else {
-      insert_group<3>(I, I.table, I.table_mask, P.k, h, l, g, cnt);
+      insert_group<3>(I.table, I.table_mask, P.k, h, l, g, bad, cnt);
     }
   }
 }
