@@ -90,6 +90,8 @@ struct InstDev {
   unsigned long long best_cand;  // min candidate index whose CS satisfies the sample (P1)
   unsigned long long best_sol;   // min candidate index of a solution owning its key
   int sol_known, pad2;           // best_sol settled before the rows were emitted
+  unsigned long long n_newlist;  // slots of keys first inserted by this level's P1 (listed in wins)
+  int attempt, attempt_level;    // attempts at the current level (> 1: a retry after growth)
   // ---- result
   int res_size, rpn_len;
   int16_t rpn[kMaxSize];

@@ -93,9 +93,11 @@ __device__ void ph_plan(const BatchDev& B, unsigned bid, unsigned nb) {
         tiles = t;
         chunks = (words + kChunkWords - 1) / kChunkWords;
         tchunks = (cap + kScanSlots - 1) / kScanSlots;
-        I.n_new = I.n_wins = I.probe_fail = 0;
+        I.n_new = I.n_wins = I.probe_fail = I.n_newlist = 0;
         I.best_cand = I.best_sol = ~0ULL;
         I.sol_known = 0;
+        I.attempt = (I.attempt_level == k) ? I.attempt + 1 : 1;
+        I.attempt_level = k;
       }
     }
     B.p1_prefix[b + 1] = tiles;
@@ -269,11 +271,15 @@ __device__ void ph_table_scan(const BatchDev& B, unsigned bid, unsigned nb) {
     const int b = find_owner(B.tscan_prefix, B.ninst, c);
     InstDev& I = B.inst[b];
     const unsigned long long k = (unsigned long long)I.level;
+    // first attempt at this level with every new slot listed: visit the list;
+    // otherwise (a retried level) scan the whole table
+    const bool listed = I.attempt == 1 && I.n_newlist <= I.tent_cap;
     const uint64_t s0 = (c - B.tscan_prefix[b]) * kScanSlots;
-    const uint64_t cap = I.table_mask + 1;
+    const uint64_t cap = listed ? I.n_newlist : I.table_mask + 1;
     const uint64_t s1 = (s0 + kScanSlots < cap) ? s0 + kScanSlots : cap;
     unsigned long long cnt = 0;
-    for (uint64_t sl = s0 + threadIdx.x; sl < s1; sl += blockDim.x) {
+    for (uint64_t e = s0 + threadIdx.x; e < s1; e += blockDim.x) {
+      const uint64_t sl = listed ? __ldcg(I.wins + e) : e;
       const unsigned long long pay = __ldcg(&I.table[sl].pay);
       if ((pay >> kPayShift) == k) {
         const uint64_t g = pay & kIdxMask;
@@ -704,7 +710,7 @@ __global__ void k_init(BatchDev* Bp) {
       uint64_t h, l;
       row_key(I, row, h, l);
       int isnew = 0;
-      const uint64_t idx = slot_hash(h, l) & I.table_mask;
+      uint64_t idx = slot_hash(h, l) & I.table_mask;
       const int r = insert_min(I.table, I.table_mask, idx, ld_key(I.table + idx), h, l, pay_of(1, v), isnew);
       if (r < 0) atomicAdd(&I.probe_fail, 1ULL);
       if (isnew) atomicAdd(&s_new, 1ULL);

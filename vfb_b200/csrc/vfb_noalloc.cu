@@ -137,6 +137,7 @@ vfb_status fill_problem(const vfb_instance& in, InstDev& d) {
   }
   d.status = ST_RUNNING;
   d.level = 1;
+  d.promote_above = ~0ULL;   // no cluster pass here: never hand the instance on
   return VFB_OK;
 }
 

@@ -31,7 +31,7 @@ __device__ __forceinline__ int claim(Slot* s, unsigned long long pay) {
 
 // Insert-or-find (h,l) starting at slot idx whose key half-words were already
 // loaded into cur.  Returns 1/0 as claim(), -1 when the probe limit is hit.
-__device__ inline int insert_min(Slot* tab, uint64_t mask, uint64_t idx, Key128 cur, uint64_t h, uint64_t l,
+__device__ inline int insert_min(Slot* tab, uint64_t mask, uint64_t& idx, Key128 cur, uint64_t h, uint64_t l,
                           unsigned long long pay, int& isnew) {
   for (int p = 0; p < kMaxProbes; ++p) {
     if (p > 0) cur = ld_key(tab + idx);
@@ -241,22 +241,43 @@ struct P1Count {
 // keys are resolved one by one.  bad[j] == 0 marks a candidate whose step-0
 // bits match every trace's label (a solution candidate).
 template <int N>
-__device__ __forceinline__ void insert_group(Slot* tab, uint64_t mask, int k, const uint64_t* h,
+__device__ __forceinline__ void insert_group(InstDev& I, unsigned live, int k, const uint64_t* h,
                                              const uint64_t* l, const uint64_t* g, const uint64_t* bad,
                                              P1Count& cnt) {
+  Slot* tab = I.table;
+  const uint64_t mask = I.table_mask;
   uint64_t idx[N];
   Key128 cur[N];
 #pragma unroll
   for (int j = 0; j < N; ++j) idx[j] = slot_hash(h[j], l[j]) & mask;
 #pragma unroll
   for (int j = 0; j < N; ++j) cur[j] = ld_key(tab + idx[j]);
+  uint64_t fresh[N];
+  int nf = 0;
 #pragma unroll
   for (int j = 0; j < N; ++j) {
     int isnew = 0;
     const int r = insert_min(tab, mask, idx[j], cur[j], h[j], l[j], pay_of(k, g[j]), isnew);
     if (r < 0) ++cnt.fail;
-    cnt.fresh += isnew;
+    if (isnew) fresh[nf++] = idx[j];
     if (!bad[j] && g[j] < cnt.sol) cnt.sol = g[j];
+  }
+  cnt.fresh += nf;
+  // list the slots of the keys this warp inserted: one atomic per warp, the
+  // per-lane offsets from three ballots of the lane's count (0..4)
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  const unsigned b0 = __ballot_sync(live, nf & 1), b1 = __ballot_sync(live, nf & 2),
+                 b2 = __ballot_sync(live, nf & 4);
+  const unsigned pre = __popc(b0 & lt) + 2 * __popc(b1 & lt) + 4 * __popc(b2 & lt);
+  const unsigned tot = __popc(b0) + 2 * __popc(b1) + 4 * __popc(b2);
+  const int leader = __ffs(live) - 1;
+  unsigned long long base = 0;
+  if (lane == leader && tot) base = atomicAdd(&I.n_newlist, (unsigned long long)tot);
+  base = __shfl_sync(live, base, leader);
+  for (int r = 0; r < nf; ++r) {
+    const unsigned long long pos = base + pre + r;
+    if (pos < I.tent_cap) I.wins[pos] = fresh[r];
   }
 }
 
@@ -267,6 +288,7 @@ __device__ __forceinline__ uint64_t pos_bit(const TileSh& P, int t) {
 template <int MODE>
 __device__ inline void p1_unary(InstDev& I, const TileSh& P, const uint64_t* sS, int sp, P1Count& cnt) {
   const uint64_t a = P.s0 + threadIdx.x;
+  const unsigned live = __ballot_sync(0xffffffffu, a < P.nS);
   if (a >= P.nS) return;
   const uint64_t* srow = sS + threadIdx.x * sp;
   KeyAcc k0, k1, k2, k3;
@@ -297,13 +319,14 @@ __device__ inline void p1_unary(InstDev& I, const TileSh& P, const uint64_t* sS,
   g[3] = I.base_g + a;
 #pragma unroll
   for (int j = 0; j < 4; ++j) bad[j] &= 1ULL;
-  insert_group<4>(I.table, I.table_mask, P.k, h, l, g, bad, cnt);
+  insert_group<4>(I, live, P.k, h, l, g, bad, cnt);
 }
 
 template <int MODE, bool FOUR>
 __device__ inline void p1_binary(InstDev& I, const TileSh& P, const uint64_t* sS, int sp, const uint64_t* sQ,
                           P1Count& cnt) {
   const uint64_t s = P.s0 + threadIdx.x;
+  const unsigned live = __ballot_sync(0xffffffffu, s < P.nS);
   if (s >= P.nS) return;
   const uint64_t* srow = sS + threadIdx.x * sp;
   const int nq = (int)((P.nQ - P.q0) < (uint64_t)P.tq ? (P.nQ - P.q0) : (uint64_t)P.tq);
@@ -345,9 +368,9 @@ __device__ inline void p1_binary(InstDev& I, const TileSh& P, const uint64_t* sS
     if (FOUR) {
       key_final<MODE>(kV, h[3], l[3]);
       g[3] = I.base_u[P.j] + b * P.ni + a;
-      insert_group<4>(I.table, I.table_mask, P.k, h, l, g, bad, cnt);
+      insert_group<4>(I, live, P.k, h, l, g, bad, cnt);
     } else {
-      insert_group<3>(I.table, I.table_mask, P.k, h, l, g, bad, cnt);
+      insert_group<3>(I, live, P.k, h, l, g, bad, cnt);
     }
   }
 }
