@@ -163,6 +163,63 @@ def run_reference(args, inst):
     print(json.dumps(line), flush=True)
 
 
+def batched(local: int, flush, count: int = 256, reps: int = 3):
+    """The mixed batch (seed 3): one vfb_batch_solve of every instance against
+    one vfb_solve per instance on the same engine, both warm (device timeline
+    of every call summed over the run, torch synchronised around it)."""
+    import torch
+    import vfb_b200
+    from vfb_b200 import synth
+    probs = [vfb_b200.Problem.from_instance(i) for i in synth.config_batch(count=count)]
+    eng = vfb_b200.Engine(device=local)
+    key = lambda r: (r.status, r.size, r.rpn, r.level_rows, r.level_cands)  # noqa: E731
+    serial = [eng.solve(p) for p in probs]        # warm-up (grows every buffer once)
+    eng.batch_solve(probs)
+    flush.zero_()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    serial = [eng.solve(p) for p in probs]
+    ts = time.perf_counter() - t0
+    tb = []
+    same = True
+    for _ in range(reps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = eng.batch_solve(probs)
+        tb.append(time.perf_counter() - t0)
+        same = same and all(key(a) == key(b) for a, b in zip(serial, out))
+    eng.close()
+    best = statistics.median(tb)
+    return {"workload": f"mixed batch: {count} planted instances (seed 3), APs 2-8, traces 4-63, "
+                        "lengths 4-64 per trace, planted size 5-11, max size planted+4",
+            "solves_per_s": count / best, "ms_per_batch": 1e3 * best,
+            "serial_solves_per_s": count / ts, "serial_ms": 1e3 * ts,
+            "speedup_vs_serial": ts / best, "identical_to_serial": same,
+            "unique_cs": sum(r.total_rows for r in serial), "reps": reps}
+
+
+def large_roofline(local: int, peak: float):
+    """Per-kernel profile of the largest instance of the mixed batch (#2,
+    11.3M unique CS): the kernels' rates on levels that fill the GPU."""
+    import vfb_b200
+    from vfb_b200 import synth
+    p = vfb_b200.Problem.from_instance(synth.config_batch(count=3)[2])
+    eng = vfb_b200.Engine(device=local, profile=True)
+    eng.solve(p)
+    eng.solve(p)
+    eng.profile_reset()
+    r = eng.solve(p)
+    prof = eng.profile()
+    eng.close()
+    name, nl, ms, nbytes = max(prof, key=lambda q: q[2])
+    achieved = nbytes / (ms * 1e-3) / 1e9
+    return {"instance": "mixed batch #2 (7 APs, 36 traces, size 9, 11.3M unique CS)",
+            "kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "ms": ms, "launches": nl, "unique_cs": r.total_rows,
+            "kernels": {q[0]: round(q[2], 3) for q in prof}}
+
+
 def cpu_baseline(inst, budget_s: float):
     import oracle
     prob = oracle.Problem.from_instance(inst, threads=1)
@@ -286,6 +343,8 @@ def main():
         "kernels": [{"name": p[0], "launches": p[1], "ms": p[2], "bytes": p[3]} for p in prof],
         "clocks": clk.summary(),
     }
+    line["batched"] = batched(local, flush)
+    line["large_instance"] = large_roofline(local, peak)
     line["cpu_baseline"] = cpu_baseline(inst, args.cpu_budget)
     print(json.dumps(line), flush=True)
     if world > 1:
