@@ -121,6 +121,26 @@ vfb_status vfb_batch_solve(void *ctx, const vfb_instance *inst, int n, vfb_resul
 #define VFB_NOALLOC_SCRATCH_BYTES (64u << 20)
 vfb_status vfb_solve_noalloc(const vfb_instance *inst, vfb_result *out);
 
+/* ------------------------------------------------------------ serving loop
+ * Continuous batching (no counterpart in the reference, which solves one
+ * instance per process).  vfb_serve_open keeps `slots` instances resident on
+ * the device (traces up to max_traces).  vfb_serve_submit queues a request
+ * (the instance is copied).  Each vfb_serve_step admits queued requests into
+ * free slots while the device memory held stays under a fraction of the
+ * budget, builds one more level of every resident instance, and returns the
+ * finished ones (up to cap) with their tags; results equal vfb_solve's.
+ * *active / *queued (may be NULL) report the slots in use and the requests
+ * waiting.  A request that cannot be admitted finishes with its status. */
+typedef struct {
+  uint64_t tag;
+  vfb_result result;
+} vfb_served;
+
+vfb_status vfb_serve_open(void *ctx, int slots, int max_traces);
+vfb_status vfb_serve_submit(void *ctx, const vfb_instance *inst, uint64_t tag);
+vfb_status vfb_serve_step(void *ctx, vfb_served *done, int cap, int *ndone, int *active, int *queued);
+void vfb_serve_close(void *ctx);
+
 /* Per-kernel profile accumulated since vfb_create (profile=1 only).  name,
  * number of launches, total device milliseconds (CUDA events around each
  * launch) and the algorithmic bytes those launches had to move (operand rows

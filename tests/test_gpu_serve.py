@@ -1,0 +1,44 @@
+"""Serving loop: requests admitted while others are on the GPU get exactly the
+result a solo vfb_solve gives."""
+import pytest
+
+import vfb_b200
+from vfb_b200 import serve, synth
+from tests import cases
+
+pytestmark = pytest.mark.gpu
+
+
+def _key(r):
+    return (r.status, r.size, r.rpn, r.level_rows, r.level_cands, r.solution_index)
+
+
+def test_stream_results_equal_solo(engine):
+    # a dense stream (all arrivals within a few ms) so requests overlap on the device
+    stream = serve.request_stream(seed=11, count=40, rate=20000.0, large_frac=0.0)
+    # one large-shape request of moderate size (8 APs, 63 traces of 64 steps, size 7)
+    stream.insert(5, (stream[5][0], vfb_b200.Problem.from_instance(synth.config_large(13))))
+    results, lat, span = serve.run_stream(engine, stream, slots=16)
+    assert all(r is not None for r in results)
+    for (t, prob), got in zip(stream, results):
+        assert _key(got) == _key(engine.solve(prob))
+    assert all(x >= 0 for x in lat)
+
+
+def test_more_requests_than_slots(engine):
+    insts = cases.planted_cases(6) + cases.small_exact_cases()[:6] + [synth.config_planted()]
+    stream = [(0.0, vfb_b200.Problem.from_instance(i)) for i in insts]
+    results, _, _ = serve.run_stream(engine, stream, slots=3)
+    for (t, prob), got in zip(stream, results):
+        assert _key(got) == _key(engine.solve(prob))
+
+
+def test_growth_inside_a_stream(engine):
+    inst = cases.random_instance(4242, 4, 5, 5, 16, 8)
+    inst.neg[0] = inst.pos[0]
+    big = vfb_b200.Problem.from_instance(inst)
+    small = vfb_b200.Problem.from_instance(synth.config_small())
+    stream = [(0.0, big), (0.0, small), (0.0, small)]
+    results, _, _ = serve.run_stream(engine, stream, slots=2)
+    assert _key(results[0]) == _key(engine.solve(big))
+    assert results[1].status == vfb_b200.OK and results[2].status == vfb_b200.OK

@@ -56,6 +56,10 @@ class _Result(ctypes.Structure):
                 ("kernel_launches", ctypes.c_uint64)]
 
 
+class _Served(ctypes.Structure):
+    _fields_ = [("tag", ctypes.c_uint64), ("result", _Result)]
+
+
 class _KernelStat(ctypes.Structure):
     _fields_ = [("name", ctypes.c_char * 32), ("launches", ctypes.c_uint64),
                 ("ms", ctypes.c_double), ("bytes", ctypes.c_double)]
@@ -68,7 +72,8 @@ class _JsonProblem(ctypes.Structure):
 
 EXPORTS = ["vfb_create", "vfb_destroy", "vfb_solve", "vfb_batch_solve", "vfb_status_str",
            "vfb_read_json", "vfb_json_free", "vfb_format_infix", "vfb_profile_read",
-           "vfb_profile_reset", "vfb_solve_noalloc", "vfb_synth_planted"]
+           "vfb_profile_reset", "vfb_solve_noalloc", "vfb_synth_planted", "vfb_serve_open",
+           "vfb_serve_submit", "vfb_serve_step", "vfb_serve_close"]
 
 _lib = None
 
@@ -110,6 +115,16 @@ def load_library():
     lib.vfb_profile_reset.restype = None
     lib.vfb_solve_noalloc.argtypes = [ctypes.POINTER(_Instance), ctypes.POINTER(_Result)]
     lib.vfb_solve_noalloc.restype = ctypes.c_int
+    lib.vfb_serve_open.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    lib.vfb_serve_open.restype = ctypes.c_int
+    lib.vfb_serve_submit.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Instance), ctypes.c_uint64]
+    lib.vfb_serve_submit.restype = ctypes.c_int
+    lib.vfb_serve_step.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Served), ctypes.c_int,
+                                   ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                   ctypes.POINTER(ctypes.c_int)]
+    lib.vfb_serve_step.restype = ctypes.c_int
+    lib.vfb_serve_close.argtypes = [ctypes.c_void_p]
+    lib.vfb_serve_close.restype = None
     _lib = lib
     return lib
 
@@ -256,6 +271,33 @@ class Engine:
         self._lib.vfb_solve(self._ctx, ctypes.byref(inst), ctypes.byref(res))
         del keep
         return _result(res)
+
+    # ---- serving (continuous batching)
+    def serve_open(self, slots: int = 256, max_traces: int = 64) -> None:
+        rc = self._lib.vfb_serve_open(self._ctx, slots, max_traces)
+        if rc != OK:
+            raise VfbError(f"vfb_serve_open failed: {STATUS_NAMES[rc]}")
+        self._served = (_Served * max(slots, 64))()
+
+    def serve_submit(self, prob: Problem, tag: int) -> None:
+        inst, keep = prob._cstruct()
+        rc = self._lib.vfb_serve_submit(self._ctx, ctypes.byref(inst), tag)
+        del keep
+        if rc != OK:
+            raise VfbError(f"vfb_serve_submit failed: {STATUS_NAMES[rc]}")
+
+    def serve_step(self):
+        """One admission + level step; returns ([(tag, Result)], active, queued)."""
+        nd, act, q = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        rc = self._lib.vfb_serve_step(self._ctx, self._served, len(self._served), ctypes.byref(nd),
+                                      ctypes.byref(act), ctypes.byref(q))
+        if rc != OK:
+            raise VfbError(f"vfb_serve_step failed: {STATUS_NAMES[rc]}")
+        done = [(self._served[i].tag, _result(self._served[i].result)) for i in range(nd.value)]
+        return done, act.value, q.value
+
+    def serve_close(self) -> None:
+        self._lib.vfb_serve_close(self._ctx)
 
     def batch_solve(self, probs: list) -> list:
         n = len(probs)

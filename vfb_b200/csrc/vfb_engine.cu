@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <new>
 #include <vector>
@@ -77,6 +78,7 @@ struct Engine {
   int p1_grid = 0;     // P1 CTAs
   cudaError_t last_error = cudaSuccess;
   bool use_loop = true;  // device-side while-node available
+  bool single_step = false;  // serving: one level per launch (admission between levels)
   bool use_coop = false;  // whole-GPU persistent cooperative solver (k_solve)
   int coop_grid = 0;
   bool use_cluster = false;  // cluster solver first, whole GPU for promoted instances
@@ -349,7 +351,7 @@ struct Engine {
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaGraphCreate(&graph, 0);
     if (e != cudaSuccess) return e;
-    bool loop = use_loop;
+    bool loop = use_loop && !single_step;
     if (loop) {
       cudaGraphConditionalHandle handle;
       e = cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault);
@@ -410,7 +412,7 @@ struct Engine {
   }
 
   cudaError_t run(int ninst, int p1_smem) {
-    if (use_coop) {
+    if (use_coop && !single_step) {
       if (coop_grid <= 0) return cudaErrorInvalidConfiguration;
       const unsigned int init_ctl[2] = {0u, 1u};   // error, continue
       cudaMemcpyAsync(hB.ctl + 2, init_ctl, sizeof(init_ctl), cudaMemcpyHostToDevice, stream);
@@ -427,7 +429,7 @@ struct Engine {
       return cudaSuccess;
     }
     if (!exec || exec_ninst != ninst || exec_smem != p1_smem || exec_grid != p1_grid ||
-        exec_loop != (int)use_loop) {
+        exec_loop != (int)(use_loop && !single_step)) {
       const cudaError_t e = build_graph(ninst, p1_smem);
       if (e != cudaSuccess) return e;
     }
@@ -1026,6 +1028,221 @@ struct Engine {
     }
   }
 
+  // ============================================================ serving
+  // A session keeps `cap` instance slots resident on the device.  Each step
+  // admits queued requests into free slots (while the projected memory fits),
+  // builds one level of every active instance with the captured step graph,
+  // grows buffers where asked, and hands back finished results.
+  struct Pending {
+    uint64_t tag;
+    vfb_instance in;
+    std::vector<uint64_t> words;
+    std::vector<int> lengths;
+  };
+  struct Session {
+    int cap = 0;
+    std::vector<InstHost> H;
+    std::vector<uint64_t> tag;
+    std::vector<char> busy;
+    std::deque<Pending> queue;
+    int p1_smem = 0;
+    double budget_frac = 0.6;
+  } sv;
+
+  vfb_status serve_open(int slots, int max_traces) {
+    if (slots <= 0) return VFB_BAD_INPUT;
+    if (cudaSetDevice(device) != cudaSuccess) return dev_fail(__LINE__);
+    serve_close();
+    sv.cap = slots;
+    sv.H.assign(slots, InstHost{});
+    sv.tag.assign(slots, 0);
+    sv.busy.assign(slots, 0);
+    const int tp = std::max(2, std::min(max_traces, (int)kMaxTraces) + (max_traces & 1));
+    sv.p1_smem = (kTS * (tp + 1) + kTQ * tp) * 8;
+    int occ = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_p1, kTS, sv.p1_smem);
+    p1_grid = sms * std::max(occ, 1);
+    vfb_status rc = ensure_workspace(slots, (uint64_t)slots * 8);
+    if (rc != VFB_OK) return rc;
+    std::vector<InstDev> idle(slots);
+    std::memset(idle.data(), 0, idle.size() * sizeof(InstDev));
+    if (cudaMemcpyAsync(dInst, idle.data(), idle.size() * sizeof(InstDev), cudaMemcpyHostToDevice, stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(stream) != cudaSuccess)
+      return dev_fail(__LINE__);
+    single_step = true;
+    return VFB_OK;
+  }
+
+  void serve_close() {
+    for (int i = 0; i < sv.cap; ++i)
+      if (sv.busy[i] && sv.H[i].d.rows) free_buffers(sv.H[i]);
+    sv = Session{};
+    single_step = false;
+    if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
+  }
+
+  vfb_status serve_submit(const vfb_instance* in, uint64_t tag) {
+    if (!in || !in->words || !in->lengths || in->num_traces < 1 || in->num_vars < 1) return VFB_BAD_INPUT;
+    Pending p;
+    p.tag = tag;
+    p.in = *in;
+    p.words.assign(in->words, in->words + (size_t)in->num_traces * in->num_vars);
+    p.lengths.assign(in->lengths, in->lengths + in->num_traces);
+    p.in.words = p.words.data();
+    p.in.lengths = p.lengths.data();
+    sv.queue.push_back(std::move(p));
+    sv.queue.back().in.words = sv.queue.back().words.data();
+    sv.queue.back().in.lengths = sv.queue.back().lengths.data();
+    return VFB_OK;
+  }
+
+  // Result of a finished slot (same fields as vfb_solve's).
+  void slot_result(const InstDev& d, const InstHost& H, vfb_result& r) {
+    std::memset(&r, 0, sizeof(r));
+    r.size = d.res_size;
+    const int top = std::min(d.res_size, (int)kMaxSize);
+    uint64_t tot = 0;
+    for (int k = 1; k <= top; ++k) {
+      r.level_rows[k] = d.lcount[k];
+      r.level_cands[k] = d.lcands[k];
+      tot += d.lcount[k];
+    }
+    r.total_rows = tot;
+    if (d.status == ST_FOUND) {
+      r.status = VFB_OK;
+      r.rpn_len = d.rpn_len;
+      for (int j = 0; j < d.rpn_len && j < kMaxSize; ++j) r.rpn[j] = d.rpn[j];
+      r.solution_index = d.sol_index;
+    } else if (d.status == ST_NOT_FOUND) {
+      r.status = VFB_NOT_FOUND;
+    } else {
+      r.status = H.fail != VFB_OK ? H.fail : VFB_DEVICE_ERROR;
+      if (r.size >= 1 && d.level <= r.size) {
+        r.total_rows -= r.level_rows[r.size];
+        r.level_rows[r.size] = 0;
+        r.level_cands[r.size] = 0;
+        r.size = std::max(0, r.size - 1);
+      }
+    }
+  }
+
+  vfb_status serve_step(vfb_served* done, int cap_done, int* ndone, int* active, int* queued) {
+    *ndone = 0;
+    if (sv.cap <= 0) return VFB_BAD_INPUT;
+    if (cudaSetDevice(device) != cudaSuccess) return dev_fail(__LINE__);
+    // 1. admission
+    bool admitted = false;
+    for (int i = 0; i < sv.cap && !sv.queue.empty(); ++i) {
+      if (sv.busy[i]) continue;
+      if (mem_limit && (double)held_bytes > sv.budget_frac * (double)mem_limit) break;
+      Pending& p = sv.queue.front();
+      InstHost& H = sv.H[i];
+      H = InstHost{};
+      vfb_status s = prepare(p.in, H);
+      const int tp = p.in.num_traces + (p.in.num_traces & 1);
+      if (s == VFB_OK && (kTS * (tp + 1) + kTQ * tp) * 8 > sv.p1_smem) s = VFB_LIMIT;
+      if (s == VFB_OK) {
+        Caps c{4096, 1u << 14, 1u << 14, 1u << 13};
+        c.rows = std::max<uint64_t>(c.rows, (uint64_t)H.d.A * 16);
+        H.sig = signature(p.in);
+        auto hit = hints.find(H.sig);
+        if (hit != hints.end()) c = hit->second;
+        s = alloc_buffers(H, c.rows, c.slots, c.words, c.tents);
+        H.d.promote_above = ~0ULL;
+      }
+      if (s == VFB_OK) {
+        std::vector<InstHost> one(1);
+        one[0] = H;
+        one[0].active = true;
+        s = upload_atoms(&p.in, one, 1);
+        if (s == VFB_OK &&
+            cudaMemcpyAsync(dInst + i, &H.d, sizeof(InstDev), cudaMemcpyHostToDevice, stream) != cudaSuccess)
+          s = dev_fail(__LINE__);
+        if (s == VFB_OK && cudaStreamSynchronize(stream) != cudaSuccess) s = dev_fail(__LINE__);
+      }
+      if (s != VFB_OK) {
+        // refused: report it as finished with that status
+        if (H.d.rows) free_buffers(H);
+        if (*ndone < cap_done) {
+          std::memset(&done[*ndone], 0, sizeof(vfb_served));
+          done[*ndone].tag = p.tag;
+          done[*ndone].result.status = s;
+          ++*ndone;
+        }
+        sv.queue.pop_front();
+        continue;
+      }
+      H.active = true;
+      sv.busy[i] = 1;
+      sv.tag[i] = p.tag;
+      sv.queue.pop_front();
+      admitted = true;
+    }
+    if (admitted) {
+      k_init<<<std::min(sv.cap, grid), 256, 0, stream>>>(dB);
+      ++c_launch;
+    }
+    // 2. one level for every active instance
+    int running = 0;
+    for (int i = 0; i < sv.cap; ++i) running += sv.busy[i];
+    if (running) {
+      uint64_t cn = 0;
+      for (int i = 0; i < sv.cap; ++i)
+        if (sv.busy[i]) cn += (sv.H[i].d.bitmap_words + kChunkWords - 1) / kChunkWords;
+      if (cn + sv.cap > hB.chunk_cap) {
+        const vfb_status s = ensure_workspace(sv.cap, cn + sv.cap);
+        if (s != VFB_OK) return s;
+      }
+      cudaError_t e = run(sv.cap, sv.p1_smem);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+      if (e != cudaSuccess) { last_error = e; return dev_fail(__LINE__); }
+      ++c_launch;
+    }
+    // 3. growth and 4. harvest
+    std::vector<int> fin;
+    for (int i = 0; i < sv.cap; ++i) {
+      if (!sv.busy[i]) continue;
+      const int st = h_status[i].x;
+      if (st == ST_NEED_MEM) {
+        const vfb_status g = grow(sv.H[i], i);
+        if (g != VFB_OK) {
+          sv.H[i].fail = g;
+          const int err = ST_ERROR;
+          cudaMemcpyAsync(&dInst[i].status, &err, sizeof(int), cudaMemcpyHostToDevice, stream);
+          fin.push_back(i);
+        }
+      } else if (st == ST_FOUND || st == ST_NOT_FOUND || st == ST_ERROR) {
+        fin.push_back(i);
+      }
+    }
+    for (int i : fin) {
+      if (*ndone >= cap_done) break;
+      InstDev d;
+      if (cudaMemcpyAsync(&d, dInst + i, sizeof(InstDev), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+          cudaStreamSynchronize(stream) != cudaSuccess)
+        return dev_fail(__LINE__);
+      vfb_served& out = done[(*ndone)++];
+      out.tag = sv.tag[i];
+      slot_result(d, sv.H[i], out.result);
+      if (d.status == ST_FOUND || d.status == ST_NOT_FOUND) {
+        if (hints.size() > 4096) hints.clear();
+        hints[sv.H[i].sig] = Caps{d.row_cap, d.table_mask + 1, d.bitmap_words, d.tent_cap};
+      }
+      free_buffers(sv.H[i]);
+      sv.H[i] = InstHost{};
+      sv.busy[i] = 0;
+      const int idle = ST_IDLE;
+      cudaMemcpyAsync(&dInst[i].status, &idle, sizeof(int), cudaMemcpyHostToDevice, stream);
+    }
+    cudaStreamSynchronize(stream);
+    int act = 0;
+    for (int i = 0; i < sv.cap; ++i) act += sv.busy[i];
+    if (active) *active = act;
+    if (queued) *queued = (int)sv.queue.size();
+    return VFB_OK;
+  }
+
   int profile_read(vfb_kernel_stat* outp, int cap) {
     int m = 0;
     for (int k = 0; k < KP_N && m < cap; ++k) {
@@ -1086,6 +1303,25 @@ vfb_status vfb_solve(void* ctx, const vfb_instance* inst, vfb_result* out) {
 vfb_status vfb_batch_solve(void* ctx, const vfb_instance* inst, int n, vfb_result* out) {
   if (!ctx || (n > 0 && (!inst || !out)) || n < 0) return VFB_BAD_INPUT;
   return static_cast<Engine*>(ctx)->batch(inst, n, out);
+}
+
+vfb_status vfb_serve_open(void* ctx, int slots, int max_traces) {
+  if (!ctx) return VFB_BAD_INPUT;
+  return static_cast<Engine*>(ctx)->serve_open(slots, max_traces);
+}
+
+vfb_status vfb_serve_submit(void* ctx, const vfb_instance* inst, uint64_t tag) {
+  if (!ctx) return VFB_BAD_INPUT;
+  return static_cast<Engine*>(ctx)->serve_submit(inst, tag);
+}
+
+vfb_status vfb_serve_step(void* ctx, vfb_served* done, int cap, int* ndone, int* active, int* queued) {
+  if (!ctx || !done || !ndone || cap <= 0) return VFB_BAD_INPUT;
+  return static_cast<Engine*>(ctx)->serve_step(done, cap, ndone, active, queued);
+}
+
+void vfb_serve_close(void* ctx) {
+  if (ctx) static_cast<Engine*>(ctx)->serve_close();
 }
 
 int vfb_profile_read(void* ctx, vfb_kernel_stat* out, int cap) {

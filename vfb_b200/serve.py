@@ -1,0 +1,89 @@
+"""Serving loop: continuous batching of arriving solve requests.
+
+run_stream() replays a request stream -- (arrival time in seconds, Problem)
+pairs -- against one engine in real time: a request is submitted once the wall
+clock passes its arrival time, every vfb_serve_step admits queued requests
+into free device slots (while the memory held stays under budget) and builds
+one more level of every resident instance, and finished results come back
+with their tags.  Requests that arrive while others are on the GPU join at the
+next level boundary.  Latency = completion time - arrival time.
+
+  python -m vfb_b200.serve --rate 100 --count 2000 [--slots 256]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import statistics
+import time
+
+from . import Engine, Problem, synth
+
+
+def percentile(xs, q):
+    xs = sorted(xs)
+    if not xs:
+        return None
+    i = min(len(xs) - 1, max(0, int(round(q / 100.0 * (len(xs) - 1)))))
+    return xs[i]
+
+
+def run_stream(engine: Engine, stream, slots: int = 256, max_traces: int = 64):
+    """Returns (results by index, latencies by index, makespan seconds)."""
+    engine.serve_open(slots, max_traces)
+    n = len(stream)
+    results, finish = [None] * n, [0.0] * n
+    nxt, done = 0, 0
+    t0 = time.perf_counter()
+    try:
+        while done < n:
+            now = time.perf_counter() - t0
+            while nxt < n and stream[nxt][0] <= now:
+                engine.serve_submit(stream[nxt][1], nxt)
+                nxt += 1
+            out, active, queued = engine.serve_step()
+            t = time.perf_counter() - t0
+            for tag, res in out:
+                results[tag] = res
+                finish[tag] = t
+                done += 1
+            if active == 0 and queued == 0 and nxt < n:
+                # idle until the next arrival
+                wait = stream[nxt][0] - (time.perf_counter() - t0)
+                if wait > 0:
+                    time.sleep(min(wait, 0.001))
+    finally:
+        engine.serve_close()
+    lat = [finish[i] - stream[i][0] for i in range(n)]
+    return results, lat, time.perf_counter() - t0
+
+
+def request_stream(seed: int = 4, count: int = 2000, rate: float = 100.0, large_frac: float = 0.05):
+    """(arrival, Problem) pairs: 95% mixed-batch shapes, 5% the large shape."""
+    return [(t, Problem.from_instance(inst))
+            for t, inst in synth.config_serving(seed, count, rate, large_frac)]
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--rate", type=float, default=100.0)
+    ap.add_argument("--count", type=int, default=2000)
+    ap.add_argument("--slots", type=int, default=256)
+    ap.add_argument("--seed", type=int, default=4)
+    args = ap.parse_args()
+    stream = request_stream(args.seed, args.count, args.rate)
+    eng = Engine()
+    # warm the kernels (module load, graph capture) outside the measured stream
+    run_stream(eng, stream[:4], args.slots)
+    res, lat, span = run_stream(eng, stream, args.slots)
+    eng.close()
+    ok = sum(1 for r in res if r is not None and r.status in (0, 1))
+    print(json.dumps({
+        "rate_req_per_s": args.rate, "requests": args.count, "completed": ok,
+        "p50_ms": 1e3 * percentile(lat, 50), "p95_ms": 1e3 * percentile(lat, 95),
+        "p99_ms": 1e3 * percentile(lat, 99), "mean_ms": 1e3 * statistics.mean(lat),
+        "solves_per_s": args.count / span, "makespan_s": span, "slots": args.slots}))
+
+
+if __name__ == "__main__":
+    main()
