@@ -126,17 +126,25 @@ vfb_status vfb_solve_noalloc(const vfb_instance *inst, vfb_result *out);
  * instance per process).  vfb_serve_open keeps `slots` instances resident on
  * the device (traces up to max_traces).  vfb_serve_submit queues a request
  * (the instance is copied).  Each vfb_serve_step admits queued requests into
- * free slots while the device memory held stays under a fraction of the
- * budget, builds one more level of every resident instance, and returns the
- * finished ones (up to cap) with their tags; results equal vfb_solve's.
+ * free slots while the bytes the resident instances are projected to hold
+ * after their next level (last level-over-level growth) stay under
+ * budget_frac of the memory budget (the head of the queue is admitted
+ * whenever no slot is busy), builds one more level of every resident
+ * instance, and returns the finished ones (up to cap) with their tags;
+ * results equal vfb_solve's.  An instance whose buffers would grow past
+ * request_bytes finishes with VFB_LIMIT and the sizes it completed.
  * *active / *queued (may be NULL) report the slots in use and the requests
- * waiting.  A request that cannot be admitted finishes with its status. */
+ * waiting.  A request that cannot be admitted finishes with its status.
+ * vfb_serve_limits sets budget_frac (default 0.8) and request_bytes (0, the
+ * default: a quarter of the budget) for the next vfb_serve_open and the
+ * open session. */
 typedef struct {
   uint64_t tag;
   vfb_result result;
 } vfb_served;
 
 vfb_status vfb_serve_open(void *ctx, int slots, int max_traces);
+vfb_status vfb_serve_limits(void *ctx, double budget_frac, uint64_t request_bytes);
 vfb_status vfb_serve_submit(void *ctx, const vfb_instance *inst, uint64_t tag);
 vfb_status vfb_serve_step(void *ctx, vfb_served *done, int cap, int *ndone, int *active, int *queued);
 void vfb_serve_close(void *ctx);

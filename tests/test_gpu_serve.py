@@ -42,3 +42,34 @@ def test_growth_inside_a_stream(engine):
     results, _, _ = serve.run_stream(engine, stream, slots=2)
     assert _key(results[0]) == _key(engine.solve(big))
     assert results[1].status == vfb_b200.OK and results[2].status == vfb_b200.OK
+
+
+def test_request_cap_ends_with_limit(engine):
+    inst = cases.random_instance(4242, 4, 5, 5, 16, 8)
+    inst.neg[0] = inst.pos[0]          # unsatisfiable: grows to max_size
+    big = vfb_b200.Problem.from_instance(inst)
+    small = vfb_b200.Problem.from_instance(synth.config_small())
+    solo = engine.solve(big)
+    try:
+        engine.serve_limits(0.8, 1 << 20)
+        results, _, _ = serve.run_stream(engine, [(0.0, big), (0.0, small)], slots=2)
+    finally:
+        engine.serve_limits(0.8, 0)
+    got = results[0]
+    assert got.status == vfb_b200.LIMIT
+    assert 1 <= got.size < solo.size
+    assert got.level_rows == solo.level_rows[:got.size]
+    assert _key(results[1]) == _key(engine.solve(small))
+
+
+def test_tight_budget_still_progresses(engine):
+    # a budget every request exceeds: one request at a time, all complete
+    insts = cases.planted_cases(4) + [synth.config_planted()]
+    stream = [(0.0, vfb_b200.Problem.from_instance(i)) for i in insts]
+    try:
+        engine.serve_limits(1e-9, 0)
+        results, _, _ = serve.run_stream(engine, stream, slots=4)
+    finally:
+        engine.serve_limits(0.8, 0)
+    for (t, prob), got in zip(stream, results):
+        assert _key(got) == _key(engine.solve(prob))

@@ -73,7 +73,7 @@ class _JsonProblem(ctypes.Structure):
 EXPORTS = ["vfb_create", "vfb_destroy", "vfb_solve", "vfb_batch_solve", "vfb_status_str",
            "vfb_read_json", "vfb_json_free", "vfb_format_infix", "vfb_profile_read",
            "vfb_profile_reset", "vfb_solve_noalloc", "vfb_synth_planted", "vfb_serve_open",
-           "vfb_serve_submit", "vfb_serve_step", "vfb_serve_close"]
+           "vfb_serve_limits", "vfb_serve_submit", "vfb_serve_step", "vfb_serve_close"]
 
 _lib = None
 
@@ -117,6 +117,8 @@ def load_library():
     lib.vfb_solve_noalloc.restype = ctypes.c_int
     lib.vfb_serve_open.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     lib.vfb_serve_open.restype = ctypes.c_int
+    lib.vfb_serve_limits.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_uint64]
+    lib.vfb_serve_limits.restype = ctypes.c_int
     lib.vfb_serve_submit.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Instance), ctypes.c_uint64]
     lib.vfb_serve_submit.restype = ctypes.c_int
     lib.vfb_serve_step.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Served), ctypes.c_int,
@@ -273,6 +275,12 @@ class Engine:
         return _result(res)
 
     # ---- serving (continuous batching)
+    def serve_limits(self, budget_frac: float = 0.8, request_bytes: int = 0) -> None:
+        """Admission fraction of the memory budget and per-request byte cap (0: budget / 4)."""
+        rc = self._lib.vfb_serve_limits(self._ctx, budget_frac, request_bytes)
+        if rc != OK:
+            raise VfbError(f"vfb_serve_limits failed: {STATUS_NAMES[rc]}")
+
     def serve_open(self, slots: int = 256, max_traces: int = 64) -> None:
         rc = self._lib.vfb_serve_open(self._ctx, slots, max_traces)
         if rc != OK:

@@ -109,7 +109,8 @@ struct Engine {
   // device block cache: size -> blocks
   std::multimap<size_t, void*> free_blocks;
   std::map<void*, size_t> live_blocks;
-  size_t held_bytes = 0;  // live + cached
+  size_t held_bytes = 0;    // live + cached
+  size_t cached_bytes = 0;  // blocks in free_blocks
 
   // per-call counters
   uint64_t c_h2d = 0, c_d2h = 0, c_launch = 0;
@@ -139,6 +140,7 @@ struct Engine {
     free_blocks.clear();
     for (auto& kv : live_blocks) cudaFree(kv.first);
     live_blocks.clear();
+    held_bytes = cached_bytes = 0;
     if (h_status) cudaFreeHost(h_status);
     h_status = nullptr;
     if (h_stage) cudaFreeHost(h_stage);
@@ -184,6 +186,7 @@ struct Engine {
     if (it != free_blocks.end() && it->first <= 4 * bytes) {
       void* p = it->second;
       *got = it->first;
+      cached_bytes -= it->first;
       free_blocks.erase(it);
       live_blocks[p] = *got;
       return p;
@@ -193,6 +196,7 @@ struct Engine {
       auto big = std::prev(free_blocks.end());
       cudaFreeAsync(big->second, stream);
       held_bytes -= big->first;
+      cached_bytes -= big->first;
       free_blocks.erase(big);
     }
     if (mem_limit && held_bytes + bytes > mem_limit) return nullptr;
@@ -211,6 +215,7 @@ struct Engine {
     auto it = live_blocks.find(p);
     if (it == live_blocks.end()) return;
     free_blocks.emplace(it->second, p);
+    cached_bytes += it->second;
     live_blocks.erase(it);
   }
 
@@ -616,7 +621,34 @@ struct Engine {
   }
 
   // Grow whatever the device asked for; the level is then re-run.
-  vfb_status grow(InstHost& H, int idx) {
+  // Device bytes the buffers of one instance occupy.
+  static uint64_t inst_bytes(const InstDev& d) {
+    return d.row_cap * ((uint64_t)d.TP * 8 + 8) + (d.table_mask + 1) * sizeof(Slot) + d.bitmap_words * 4 +
+           d.tent_cap * 8;
+  }
+
+  // Bytes an instance is expected to hold once its next level is built: the
+  // next level's rows are projected from the last level-over-level growth
+  // (clamped to [1, 32]); rows, table slots (kept at most half full) and the
+  // owner list scale with them.
+  static uint64_t projected_bytes(const InstDev& d) {
+    const uint64_t held = inst_bytes(d);
+    const int k = d.level;
+    if (d.status != ST_RUNNING && d.status != ST_NEED_MEM) return held;
+    if (k < 2 || k > (int)kMaxSize) return held;
+    const uint64_t last = d.lcount[k - 1], prev = k >= 3 ? d.lcount[k - 2] : d.A;
+    double ratio = prev ? (double)last / (double)prev : 1.0;
+    ratio = std::min(32.0, std::max(1.0, ratio));
+    const uint64_t next = (uint64_t)((double)last * ratio);
+    const uint64_t rows = d.lstart[k - 1] + last + next;
+    const uint64_t est = rows * ((uint64_t)d.TP * 8 + 8) + pow2_at_least(2 * (d.keys + next)) * sizeof(Slot) +
+                         d.bitmap_words * 4 + next * 8;
+    return std::max(held, est);
+  }
+
+  // cap_bytes > 0: the instance may hold at most that many bytes; a growth
+  // past it ends the instance with VFB_LIMIT.
+  vfb_status grow(InstHost& H, int idx, uint64_t cap_bytes = 0) {
     ++c_grow;
     InstDev& d = H.d;
     if (cudaMemcpyAsync(&d, dInst + idx, sizeof(InstDev), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
@@ -632,6 +664,16 @@ struct Engine {
                    (unsigned long long)d.need_amount[0], (unsigned long long)d.need_amount[2]);
     if (need & NEED_LIMIT) return VFB_LIMIT;
     if (need & NEED_PROMOTE) d.promote_above = ~0ULL;   // continue on the whole GPU
+    if (cap_bytes) {
+      uint64_t add = 0;
+      if (need & NEED_ROWS)
+        add += std::max<uint64_t>(2 * d.row_cap, d.need_amount[3] + d.need_amount[3] / 4) * ((uint64_t)d.TP * 8 + 8);
+      if (need & NEED_TABLE)
+        add += pow2_at_least(std::max<uint64_t>(2 * (d.table_mask + 1), d.need_amount[1])) * sizeof(Slot);
+      if (need & NEED_BITMAP) add += std::max<uint64_t>(2 * d.bitmap_words, d.need_amount[0] + d.need_amount[0] / 4) * 4;
+      if (need & NEED_LIST) add += std::max<uint64_t>(2 * d.tent_cap, d.need_amount[2] + d.need_amount[2] / 4) * 8;
+      if (inst_bytes(d) + add > cap_bytes) return VFB_LIMIT;
+    }
     if (need & NEED_ROWS) {
       const uint64_t want = std::max<uint64_t>(2 * d.row_cap, d.need_amount[3] + d.need_amount[3] / 4);
       const uint64_t used = d.lstart[d.level];
@@ -1045,9 +1087,24 @@ struct Engine {
     std::vector<uint64_t> tag;
     std::vector<char> busy;
     std::deque<Pending> queue;
+    std::vector<uint64_t> proj;   // projected bytes of each busy slot after its next level
+    InstDev* h_inst = nullptr;    // pinned mirror of the slot records
     int p1_smem = 0;
-    double budget_frac = 0.6;
+    double budget_frac = 0.8;     // admission: projected bytes of all slots <= budget_frac * budget
+    uint64_t request_bytes = 0;   // per-request cap (0: a quarter of the budget)
   } sv;
+
+  // Admission fraction and per-request byte cap of the serving session.
+  vfb_status serve_limits(double budget_frac, uint64_t request_bytes) {
+    if (!(budget_frac > 0.0 && budget_frac <= 1.0)) return VFB_BAD_INPUT;
+    sv_budget_frac = budget_frac;
+    sv_request_bytes = request_bytes;
+    sv.budget_frac = budget_frac;
+    sv.request_bytes = request_bytes;
+    return VFB_OK;
+  }
+  double sv_budget_frac = 0.8;
+  uint64_t sv_request_bytes = 0;
 
   vfb_status serve_open(int slots, int max_traces) {
     if (slots <= 0) return VFB_BAD_INPUT;
@@ -1057,6 +1114,13 @@ struct Engine {
     sv.H.assign(slots, InstHost{});
     sv.tag.assign(slots, 0);
     sv.busy.assign(slots, 0);
+    sv.proj.assign(slots, 0);
+    sv.budget_frac = sv_budget_frac;
+    sv.request_bytes = sv_request_bytes ? sv_request_bytes : (uint64_t)(mem_limit / 4);
+    if (cudaMallocHost(&sv.h_inst, (size_t)slots * sizeof(InstDev)) != cudaSuccess) {
+      sv.h_inst = nullptr;
+      return VFB_OOM;
+    }
     const int tp = std::max(2, std::min(max_traces, (int)kMaxTraces) + (max_traces & 1));
     sv.p1_smem = (kTS * (tp + 1) + kTQ * tp) * 8;
     int occ = 1;
@@ -1077,6 +1141,7 @@ struct Engine {
   void serve_close() {
     for (int i = 0; i < sv.cap; ++i)
       if (sv.busy[i] && sv.H[i].d.rows) free_buffers(sv.H[i]);
+    if (sv.h_inst) cudaFreeHost(sv.h_inst);
     sv = Session{};
     single_step = false;
     if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
@@ -1131,11 +1196,17 @@ struct Engine {
     *ndone = 0;
     if (sv.cap <= 0) return VFB_BAD_INPUT;
     if (cudaSetDevice(device) != cudaSuccess) return dev_fail(__LINE__);
-    // 1. admission
+    // 1. admission, while the projected bytes of all slots fit the budget;
+    // with no slot busy the head of the queue is always admitted
     bool admitted = false;
+    uint64_t committed = 0;
+    int nbusy = 0;
+    for (int i = 0; i < sv.cap; ++i)
+      if (sv.busy[i]) { committed += sv.proj[i]; ++nbusy; }
+    const double budget = sv.budget_frac * (double)mem_limit;
     for (int i = 0; i < sv.cap && !sv.queue.empty(); ++i) {
       if (sv.busy[i]) continue;
-      if (mem_limit && (double)held_bytes > sv.budget_frac * (double)mem_limit) break;
+      if (mem_limit && nbusy > 0 && (double)committed > budget) break;
       Pending& p = sv.queue.front();
       InstHost& H = sv.H[i];
       H = InstHost{};
@@ -1147,7 +1218,11 @@ struct Engine {
         c.rows = std::max<uint64_t>(c.rows, (uint64_t)H.d.A * 16);
         H.sig = signature(p.in);
         auto hit = hints.find(H.sig);
-        if (hit != hints.end()) c = hit->second;
+        if (hit != hints.end()) {
+          const Caps& h = hit->second;
+          const uint64_t hb = h.rows * ((uint64_t)H.d.TP * 8 + 8) + h.slots * sizeof(Slot) + h.words * 4 + h.tents * 8;
+          if (hb <= sv.request_bytes) c = h;
+        }
         s = alloc_buffers(H, c.rows, c.slots, c.words, c.tents);
         H.d.promote_above = ~0ULL;
       }
@@ -1176,6 +1251,9 @@ struct Engine {
       H.active = true;
       sv.busy[i] = 1;
       sv.tag[i] = p.tag;
+      sv.proj[i] = inst_bytes(H.d);
+      committed += sv.proj[i];
+      ++nbusy;
       sv.queue.pop_front();
       admitted = true;
     }
@@ -1205,7 +1283,7 @@ struct Engine {
       if (!sv.busy[i]) continue;
       const int st = h_status[i].x;
       if (st == ST_NEED_MEM) {
-        const vfb_status g = grow(sv.H[i], i);
+        const vfb_status g = grow(sv.H[i], i, sv.request_bytes);
         if (g != VFB_OK) {
           sv.H[i].fail = g;
           const int err = ST_ERROR;
@@ -1235,9 +1313,19 @@ struct Engine {
       const int idle = ST_IDLE;
       cudaMemcpyAsync(&dInst[i].status, &idle, sizeof(int), cudaMemcpyHostToDevice, stream);
     }
-    cudaStreamSynchronize(stream);
+    // 5. projections for the next admission (only needed while requests wait)
     int act = 0;
     for (int i = 0; i < sv.cap; ++i) act += sv.busy[i];
+    if (act && !sv.queue.empty() && mem_limit) {
+      if (cudaMemcpyAsync(sv.h_inst, dInst, (size_t)sv.cap * sizeof(InstDev), cudaMemcpyDeviceToHost, stream) !=
+          cudaSuccess)
+        return dev_fail(__LINE__);
+      if (cudaStreamSynchronize(stream) != cudaSuccess) return dev_fail(__LINE__);
+      for (int i = 0; i < sv.cap; ++i)
+        if (sv.busy[i]) sv.proj[i] = projected_bytes(sv.h_inst[i]);
+    } else {
+      cudaStreamSynchronize(stream);
+    }
     if (active) *active = act;
     if (queued) *queued = (int)sv.queue.size();
     return VFB_OK;
@@ -1308,6 +1396,11 @@ vfb_status vfb_batch_solve(void* ctx, const vfb_instance* inst, int n, vfb_resul
 vfb_status vfb_serve_open(void* ctx, int slots, int max_traces) {
   if (!ctx) return VFB_BAD_INPUT;
   return static_cast<Engine*>(ctx)->serve_open(slots, max_traces);
+}
+
+vfb_status vfb_serve_limits(void* ctx, double budget_frac, uint64_t request_bytes) {
+  if (!ctx) return VFB_BAD_INPUT;
+  return static_cast<Engine*>(ctx)->serve_limits(budget_frac, request_bytes);
 }
 
 vfb_status vfb_serve_submit(void* ctx, const vfb_instance* inst, uint64_t tag) {

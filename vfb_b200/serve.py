@@ -9,6 +9,12 @@ with their tags.  Requests that arrive while others are on the GPU join at the
 next level boundary.  Latency = completion time - arrival time.
 
   python -m vfb_b200.serve --rate 100 --count 2000 [--slots 256]
+  python -m vfb_b200.serve --rates 10,20,50,100,200,500 --window 20
+
+Large-shape requests (8 APs, 63 traces of length 64) grow until their buffers
+reach the per-request cap (--request-gb, default a quarter of the budget) and
+then finish with status LIMIT and the sizes they completed; the output counts
+them apart from the solved ones.
 """
 from __future__ import annotations
 
@@ -64,25 +70,41 @@ def request_stream(seed: int = 4, count: int = 2000, rate: float = 100.0, large_
             for t, inst in synth.config_serving(seed, count, rate, large_frac)]
 
 
+def summarize(rate, res, lat, span, slots):
+    by = {}
+    for r in res:
+        name = "missing" if r is None else {0: "found", 1: "not_found", 2: "limit", 3: "oom"}.get(
+            r.status, "error")
+        by[name] = by.get(name, 0) + 1
+    return {"rate_req_per_s": rate, "requests": len(res), "status": by,
+            "p50_ms": 1e3 * percentile(lat, 50), "p95_ms": 1e3 * percentile(lat, 95),
+            "p99_ms": 1e3 * percentile(lat, 99), "mean_ms": 1e3 * statistics.mean(lat),
+            "solves_per_s": len(res) / span, "makespan_s": span, "slots": slots}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--rate", type=float, default=100.0)
+    ap.add_argument("--rates", type=str, default="",
+                    help="comma-separated sweep; each rate replays min(count, window*rate) requests")
+    ap.add_argument("--window", type=float, default=20.0, help="seconds of arrivals per swept rate")
     ap.add_argument("--count", type=int, default=2000)
     ap.add_argument("--slots", type=int, default=256)
     ap.add_argument("--seed", type=int, default=4)
+    ap.add_argument("--large-frac", type=float, default=0.05)
+    ap.add_argument("--request-gb", type=float, default=0.0, help="per-request cap (0: budget / 4)")
     args = ap.parse_args()
-    stream = request_stream(args.seed, args.count, args.rate)
+    rates = [float(x) for x in args.rates.split(",")] if args.rates else [args.rate]
     eng = Engine()
-    # warm the kernels (module load, graph capture) outside the measured stream
-    run_stream(eng, stream[:4], args.slots)
-    res, lat, span = run_stream(eng, stream, args.slots)
+    eng.serve_limits(0.8, int(args.request_gb * (1 << 30)))
+    for rate in rates:
+        count = args.count if not args.rates else min(args.count, max(50, int(args.window * rate)))
+        stream = request_stream(args.seed, count, rate, args.large_frac)
+        # warm the kernels (module load, graph capture) outside the measured stream
+        run_stream(eng, [(0.0, p) for _, p in stream[:4] if p.num_traces < 63] or stream[:1], args.slots)
+        res, lat, span = run_stream(eng, stream, args.slots)
+        print(json.dumps(summarize(rate, res, lat, span, args.slots)), flush=True)
     eng.close()
-    ok = sum(1 for r in res if r is not None and r.status in (0, 1))
-    print(json.dumps({
-        "rate_req_per_s": args.rate, "requests": args.count, "completed": ok,
-        "p50_ms": 1e3 * percentile(lat, 50), "p95_ms": 1e3 * percentile(lat, 95),
-        "p99_ms": 1e3 * percentile(lat, 99), "mean_ms": 1e3 * statistics.mean(lat),
-        "solves_per_s": args.count / span, "makespan_s": span, "slots": args.slots}))
 
 
 if __name__ == "__main__":
