@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include")]
 
 UNITS = ["vfb_kernels.cu", "vfb_engine.cu", "vfb_io.cpp", "vfb_noalloc.cu", "vfb_synth.cpp"]
-HEADERS = ["vfb_device.cuh", "vfb_kernels.cuh"]
+HEADERS = ["vfb_device.cuh", "vfb_kernels.cuh", "vfb_ops.cuh"]
 
 
 def _newer(target: str, deps: list[str]) -> bool:

@@ -92,6 +92,9 @@ struct InstDev {
   int sol_known, pad2;           // best_sol settled before the rows were emitted
   unsigned long long n_newlist;  // slots of keys first inserted by this level's P1 (listed in wins)
   int attempt, attempt_level;    // attempts at the current level (> 1: a retry after growth)
+  int planned, pad3;             // level the current plan (bases, tiling) was made for; 0: none
+  unsigned long long plan_tiles, plan_words, plan_tchunks;   // P1 tiles, bitmap words, table-scan
+                                                             // chunks of the current plan
   // ---- result
   int res_size, rpn_len;
   int16_t rpn[kMaxSize];

@@ -50,12 +50,14 @@ uint64_t pow2_at_most(uint64_t x) {
 }
 
 // Kernels of one level step, in launch order (ids index Engine::prof).
-enum KId { KP_PLAN, KP_P1, KP_TSCAN, KP_COUNT, KP_SCAN, KP_EMIT, KP_ROWS, KP_FINISH, KP_LOOP, KP_INIT, KP_REHASH,
-           KP_N };
-const char* const kNames[KP_N] = {"k_plan", "k_p1", "k_table_scan", "k_chunk_count", "k_chunk_scan",
-                                  "k_chunk_emit", "k_emit_rows", "k_finish", "k_loop_ctl", "k_init", "k_rehash"};
-const int kStepSeq[] = {KP_PLAN, KP_P1, KP_TSCAN, KP_COUNT, KP_SCAN, KP_EMIT, KP_ROWS, KP_FINISH};
+enum KId { KP_ADVANCE, KP_P1, KP_TSCAN, KP_COMPACT, KP_EMIT, KP_INIT, KP_REHASH, KP_N };
+const char* const kNames[KP_N] = {"k_advance", "k_p1", "k_table_scan", "k_compact", "k_emit", "k_init",
+                                  "k_rehash"};
+// One launch of the step graph: plan the instances that need it, then build
+// one level (the trailing k_advance finishes it and plans the next).
+const int kStepSeq[] = {KP_ADVANCE, KP_P1, KP_TSCAN, KP_COMPACT, KP_EMIT, KP_ADVANCE};
 constexpr int kStepLen = sizeof(kStepSeq) / sizeof(int);
+constexpr int kBodyLen = 5;   // kernels of one level inside the device-side loop
 constexpr unsigned kMaxLoop = 4 * kMaxSize;
 // candidates of one level above which an instance leaves the cluster solver
 constexpr unsigned long long kPromoteAbove = 1ULL << 21;
@@ -76,6 +78,7 @@ struct Engine {
   int sms = 0;
   int grid = 0;        // grid-stride CTAs (256 threads)
   int p1_grid = 0;     // P1 CTAs
+  int adv_threads = 1024;  // k_advance threads (set per captured batch size)
   cudaError_t last_error = cudaSuccess;
   bool use_loop = true;  // device-side while-node available
   bool single_step = false;  // serving: one level per launch (admission between levels)
@@ -326,33 +329,36 @@ struct Engine {
   }
 
   // --------------------------------------------------------- step launch
-  void launch_step(int ninst, int p1_smem, bool timed) {
-    const int g = grid, gc = sms * 2;
+  // pre: the leading k_advance (plans instances coming from k_init or a
+  // growth).  loop: the trailing k_advance sets the while-node's condition.
+  void launch_step(bool pre, bool timed, int p1_smem, cudaGraphConditionalHandle handle, bool loop) {
     int e = 0;
     // external event nodes keep their timestamps inside a captured graph
     auto mark = [&]() { if (timed) cudaEventRecordWithFlags(ev_k[e++], stream, cudaEventRecordExternal); };
     mark();
-    k_plan<<<1, 1024, 0, stream>>>(dB);
-    mark();
+    if (pre) {
+      k_advance<<<1, adv_threads, 0, stream>>>(dB, handle, 0, loop ? 1 : 0, kMaxLoop);
+      mark();
+    }
     k_p1<<<p1_grid, kTS, p1_smem, stream>>>(dB);
     mark();
-    k_table_scan<<<g, 256, 0, stream>>>(dB);
+    k_table_scan_check<<<grid, 256, 0, stream>>>(dB);
     mark();
-    k_chunk_count<<<gc, 256, 0, stream>>>(dB);
+    k_compact<<<sms * 8, kCompactThreads, 0, stream>>>(dB);
     mark();
-    k_chunk_scan<<<std::min(ninst, g), kScanThreads, 0, stream>>>(dB);
+    k_emit<<<grid, 256, 0, stream>>>(dB);
     mark();
-    k_chunk_emit<<<gc, kChunkThreads, 0, stream>>>(dB);
-    mark();
-    k_emit_rows<<<g, 256, 0, stream>>>(dB);
-    mark();
-    k_finish<<<(ninst + 255) / 256, 256, 0, stream>>>(dB);
+    k_advance<<<1, adv_threads, 0, stream>>>(dB, handle, 1, loop ? 1 : 0, kMaxLoop);
     mark();
   }
 
-  // Graph: [loop: step + k_loop_ctl] + status read-back, or one step + status.
+  // Graph: [k_advance, while: (k_p1, k_table_scan_check, k_compact, k_emit, k_advance)] + status
+  // read-back, or one step [k_advance, k_p1, ..., k_advance] + status read-back.
   cudaError_t build_graph(int ninst, int p1_smem) {
     if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
+    // one thread per instance (whole warps, at most 1024): small batches keep
+    // k_advance's block scans short
+    adv_threads = std::min(1024, std::max(32, (ninst + 31) / 32 * 32));
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaGraphCreate(&graph, 0);
     if (e != cudaSuccess) return e;
@@ -365,14 +371,24 @@ struct Engine {
       cp.conditional.handle = handle;
       cp.conditional.type = cudaGraphCondTypeWhile;
       cp.conditional.size = 1;
-      cudaGraphNode_t cnode;
-      if (e == cudaSuccess) e = cudaGraphAddNode(&cnode, graph, nullptr, 0, &cp);
+      // plan node (sets the condition before the first iteration), then the loop
+      cudaGraphNode_t pnode = nullptr, cnode;
+      if (e == cudaSuccess) {
+        e = cudaStreamBeginCaptureToGraph(stream, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+          k_advance<<<1, adv_threads, 0, stream>>>(dB, handle, 0, 1, kMaxLoop);
+          cudaGraph_t out = nullptr;
+          e = cudaStreamEndCapture(stream, &out);
+        }
+        size_t nn = 1;
+        if (e == cudaSuccess) e = cudaGraphGetNodes(graph, &pnode, &nn);
+      }
+      if (e == cudaSuccess) e = cudaGraphAddNode(&cnode, graph, &pnode, 1, &cp);
       if (e == cudaSuccess) {
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         e = cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
-          launch_step(ninst, p1_smem, false);
-          k_loop_ctl<<<1, 256, 0, stream>>>(dB, handle, kMaxLoop);
+          launch_step(false, false, p1_smem, handle, true);
           cudaGraph_t out = nullptr;
           e = cudaStreamEndCapture(stream, &out);
         }
@@ -400,7 +416,7 @@ struct Engine {
     if (!loop) {
       e = cudaStreamBeginCaptureToGraph(stream, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
       if (e != cudaSuccess) { cudaGraphDestroy(graph); return e; }
-      launch_step(ninst, p1_smem, profile != 0);
+      launch_step(true, profile != 0, p1_smem, 0, false);
       cudaMemcpyAsync(h_status, hB.status_out, (size_t)ninst * sizeof(int2), cudaMemcpyDeviceToHost, stream);
       cudaGraph_t out = nullptr;
       e = cudaStreamEndCapture(stream, &out);
@@ -726,6 +742,7 @@ struct Engine {
     }
     d.status = ST_RUNNING;
     d.need = 0;
+    d.planned = 0;   // the level is planned again with the new buffers
     if (cudaMemcpyAsync(dInst + idx, &d, sizeof(InstDev), cudaMemcpyHostToDevice, stream) != cudaSuccess)
       return dev_fail(__LINE__);
     c_h2d += sizeof(InstDev);
@@ -833,9 +850,8 @@ struct Engine {
     const double w0 = std::ceil(cands / 32.0) * 4;
     prof[KP_P1].bytes += operands + 32.0 * cands;
     prof[KP_TSCAN].bytes += 32.0 * (double)(d.table_mask + 1) + 4.0 * wins;
-    prof[KP_COUNT].bytes += w0;
-    prof[KP_EMIT].bytes += 2 * w0 + 8.0 * wins;
-    if (!d.sol_known) prof[KP_ROWS].bytes += wins * (2 * T8 + 8.0 * d.TP + 16);
+    prof[KP_COMPACT].bytes += 2 * w0 + 8.0 * wins;
+    if (!d.sol_known) prof[KP_EMIT].bytes += wins * (2 * T8 + 8.0 * d.TP + 16);
   }
 
   void profile_step(int n, std::vector<InstHost>& H) {
@@ -907,7 +923,7 @@ struct Engine {
       H[i].d.promote_above = clusters ? kPromoteAbove : ~0ULL;
       if (s != VFB_OK) { H[i].fail = s; H[i].d.status = ST_IDLE; continue; }
       H[i].active = true;
-      chunk_need += (H[i].d.bitmap_words + kChunkWords - 1) / kChunkWords;
+      chunk_need += (H[i].d.bitmap_words + kCompactWords - 1) / kCompactWords;
     }
     rc = upload_atoms(ins, H, n);
     if (rc == VFB_OK) rc = ensure_workspace(n, chunk_need + n);
@@ -967,7 +983,7 @@ struct Engine {
         if (grew) {
           uint64_t cn = 0;
           for (int i = 0; i < n; ++i)
-            if (H[i].d.bitmap) cn += (H[i].d.bitmap_words + kChunkWords - 1) / kChunkWords;
+            if (H[i].d.bitmap) cn += (H[i].d.bitmap_words + kCompactWords - 1) / kCompactWords;
           if (cn + n > hB.chunk_cap) {
             rc = ensure_workspace(n, cn + n);
             if (rc != VFB_OK) break;
@@ -985,10 +1001,12 @@ struct Engine {
         c_launch += exec_loop ? 0 : (uint64_t)kStepLen;
       }
       if (!use_coop && exec_loop) {
+        // the plan node, then kBodyLen kernels per loop iteration (each
+        // k_advance counts one iteration)
         unsigned long long it = 0;
         cudaMemcpy(&it, hB.loop_iter, sizeof(it), cudaMemcpyDeviceToHost);
         c_d2h += sizeof(it);
-        c_launch += it * (kStepLen + 1);
+        c_launch += it ? 1 + (it - 1) * kBodyLen : 0;
       }
       if (profile) profile_step(n, H);
       if (verbose) report_progress(n);
@@ -1267,7 +1285,7 @@ struct Engine {
     if (running) {
       uint64_t cn = 0;
       for (int i = 0; i < sv.cap; ++i)
-        if (sv.busy[i]) cn += (sv.H[i].d.bitmap_words + kChunkWords - 1) / kChunkWords;
+        if (sv.busy[i]) cn += (sv.H[i].d.bitmap_words + kCompactWords - 1) / kCompactWords;
       if (cn + sv.cap > hB.chunk_cap) {
         const vfb_status s = ensure_workspace(sv.cap, cn + sv.cap);
         if (s != VFB_OK) return s;

@@ -1,11 +1,9 @@
 // vfb_kernels.cu -- sm_100a kernels of one level step of the cached search.
 //
-// One level k is built by this launch sequence (every kernel reads its work
-// from device memory, so the same sequence serves every level and any number
-// of instances):
+// Every kernel reads its work from device memory, so the same launch
+// sequence serves every level and any number of instances.  The graph solver
+// builds level k with
 //
-//   k_plan        per instance: candidate-block bases of level k, P1 tiling,
-//                 buffer checks                         (LTL_BS.cu:1226-1488)
 //   k_p1          every candidate: operator words -> 126-bit key -> insert
 //                 into the instance's hash set with atomicMin on the
 //                 candidate's canonical index; the smallest candidate index
@@ -16,12 +14,17 @@
 //                 seen at this level; its payload's index is the key's owner
 //                 (the minimum candidate index): set the owner's bit.  Also
 //                 settles whether the recorded solution candidate owns its key
-//   k_chunk_*     order-preserving compaction of the owner bitmap into the
-//                 ascending owner list (count per chunk / scan / emit)
-//   k_emit_rows   owners' rows appended to the level cache in canonical order,
-//                 solution test (insertInCache LTL_BS.cu:299-329); skipped
-//                 when the solution is already settled
-//   k_finish      level bookkeeping, formula reconstruction (LTL_BS.cu:561-705)
+//   k_compact     ordered compaction of the owner bitmap into the ascending
+//                 owner list and the owners' rows appended to the level cache
+//                 in canonical order, solution test (insertInCache
+//                 LTL_BS.cu:299-329); rows skipped when the solution is settled
+//   k_advance     level bookkeeping, formula reconstruction (LTL_BS.cu:561-705),
+//                 then the next level's candidate-block bases, P1 tiling and
+//                 buffer checks (LTL_BS.cu:1226-1488)
+//
+// The persistent, cluster and allocation-free solvers run the same phases
+// as k_plan, k_p1, k_table_scan, k_chunk_count/scan/emit, k_emit_rows,
+// k_finish.
 //
 // The reference's thrust::remove/copy_n compaction (storeUniqueLTLs
 // LTL_BS.cu:489-530) is replaced by the bitmap compaction; its racy
@@ -33,71 +36,87 @@
 namespace vfb {
 
 // ===================================================================== plan
+// Plan level k = I.level of a RUNNING instance: candidate-block bases, P1
+// tiling, buffer checks.  Records the plan (planned = k, plan_*) or asks the
+// host for memory (NEED_MEM, planned = 0).
+__device__ void plan_one(InstDev& I) {
+  const int k = I.level;
+  const uint64_t* n = I.lcount;
+  I.lstart[k] = I.lstart[k - 1] + n[k - 1];
+  uint64_t g = 0;
+  I.base_not = g;
+  g += n[k - 1];
+  for (int i = 1; 2 * i <= k - 1; ++i) { I.base_and[i] = g; g += n[i] * n[k - 1 - i]; }
+  for (int i = 1; 2 * i <= k - 1; ++i) { I.base_or[i] = g; g += n[i] * n[k - 1 - i]; }
+  I.base_x = g; g += n[k - 1];
+  I.base_f = g; g += n[k - 1];
+  I.base_g = g; g += n[k - 1];
+  for (int i = 1; i <= k - 2; ++i) { I.base_u[i] = g; g += n[i] * n[k - 1 - i]; }
+  I.cands = g;
+  // P1 tiling: kTS stream rows x tq staged rows per tile; small levels get
+  // shorter tiles so that they still spread over every SM
+  // (tq is a power of two: tile counts by shifts, not 64-bit divisions)
+  uint64_t t = 0;
+  int lg = 0;
+  while ((1 << (lg + 1)) <= kTQ) ++lg;
+  for (;;) {
+    t = (n[k - 1] + kTS - 1) / kTS;
+    I.grp_prefix[0] = 0;
+    I.grp_prefix[1] = t;
+    for (int i = 1; i < kGroups; ++i) {
+      if (2 * i <= k - 1) {
+        const int j = k - 1 - i;
+        const bool qleft = (i == j) || (n[i] <= n[j]);
+        const uint64_t nS = qleft ? n[j] : n[i], nQ = qleft ? n[i] : n[j];
+        const uint64_t qt = (nQ + (1ULL << lg) - 1) >> lg, st = (nS + kTS - 1) / kTS;
+        I.grp_qtiles[i] = (uint32_t)qt;
+        t += st * qt;
+      }
+      I.grp_prefix[i + 1] = t;
+    }
+    if (t >= (uint64_t)kP1TileTarget || lg == 0) break;
+    --lg;
+  }
+  I.tq = 1 << lg;
+  const uint64_t words = (g + 31) / 32;
+  const uint64_t cap = I.table_mask + 1;
+  // new keys of this level: at most all candidates; expect ~8x growth
+  const uint64_t grow = 8 * n[k - 1] + 4096;
+  const uint64_t est = g < grow ? g : grow;
+  int need = 0;
+  if (g >= (1ULL << kPayShift)) need |= NEED_LIMIT;
+  if (g > I.promote_above) need |= NEED_PROMOTE;
+  if (words > I.bitmap_words) { need |= NEED_BITMAP; I.need_amount[0] = words; }
+  if (2 * (I.keys + est) > cap) { need |= NEED_TABLE; I.need_amount[1] = 4 * (I.keys + est); }
+  if (I.lstart[k] + est > I.row_cap) { need |= NEED_ROWS; I.need_amount[3] = I.lstart[k] + est; }
+  if (est > I.tent_cap) { need |= NEED_LIST; I.need_amount[2] = est; }
+  if (need) {
+    I.status = ST_NEED_MEM;
+    I.need = need;
+    I.planned = 0;
+  } else {
+    I.plan_tiles = t;
+    I.plan_words = words;
+    I.plan_tchunks = (cap + kScanSlots - 1) / kScanSlots;
+    I.planned = k;
+    I.n_new = I.n_wins = I.probe_fail = I.n_newlist = 0;
+    I.best_cand = I.best_sol = ~0ULL;
+    I.sol_known = 0;
+    I.attempt = (I.attempt_level == k) ? I.attempt + 1 : 1;
+    I.attempt_level = k;
+  }
+}
+
 __device__ void ph_plan(const BatchDev& B, unsigned bid, unsigned nb) {
   for (int b = bid * blockDim.x + threadIdx.x; b < B.ninst; b += nb * blockDim.x) {
     InstDev& I = B.inst[b];
     unsigned long long tiles = 0, chunks = 0, tchunks = 0;
     if (I.status == ST_RUNNING) {
-      const int k = I.level;
-      const uint64_t* n = I.lcount;
-      I.lstart[k] = I.lstart[k - 1] + n[k - 1];
-      uint64_t g = 0;
-      I.base_not = g;
-      g += n[k - 1];
-      for (int i = 1; 2 * i <= k - 1; ++i) { I.base_and[i] = g; g += n[i] * n[k - 1 - i]; }
-      for (int i = 1; 2 * i <= k - 1; ++i) { I.base_or[i] = g; g += n[i] * n[k - 1 - i]; }
-      I.base_x = g; g += n[k - 1];
-      I.base_f = g; g += n[k - 1];
-      I.base_g = g; g += n[k - 1];
-      for (int i = 1; i <= k - 2; ++i) { I.base_u[i] = g; g += n[i] * n[k - 1 - i]; }
-      I.cands = g;
-      // P1 tiling: kTS stream rows x tq staged rows per tile; small levels get
-      // shorter tiles so that they still spread over every SM
-      uint64_t t = 0;
-      int tq = kTQ;
-      for (;;) {
-        t = (n[k - 1] + kTS - 1) / kTS;
-        I.grp_prefix[0] = 0;
-        I.grp_prefix[1] = t;
-        for (int i = 1; i < kGroups; ++i) {
-          if (2 * i <= k - 1) {
-            const int j = k - 1 - i;
-            const bool qleft = (i == j) || (n[i] <= n[j]);
-            const uint64_t nS = qleft ? n[j] : n[i], nQ = qleft ? n[i] : n[j];
-            const uint64_t qt = (nQ + tq - 1) / tq, st = (nS + kTS - 1) / kTS;
-            I.grp_qtiles[i] = (uint32_t)qt;
-            t += st * qt;
-          }
-          I.grp_prefix[i + 1] = t;
-        }
-        if (t >= (uint64_t)kP1TileTarget || tq == 1) break;
-        tq >>= 1;
-      }
-      I.tq = tq;
-      const uint64_t words = (g + 31) / 32;
-      const uint64_t cap = I.table_mask + 1;
-      // new keys of this level: at most all candidates; expect ~8x growth
-      const uint64_t grow = 8 * n[k - 1] + 4096;
-      const uint64_t est = g < grow ? g : grow;
-      int need = 0;
-      if (g >= (1ULL << kPayShift)) need |= NEED_LIMIT;
-      if (g > I.promote_above) need |= NEED_PROMOTE;
-      if (words > I.bitmap_words) { need |= NEED_BITMAP; I.need_amount[0] = words; }
-      if (2 * (I.keys + est) > cap) { need |= NEED_TABLE; I.need_amount[1] = 4 * (I.keys + est); }
-      if (I.lstart[k] + est > I.row_cap) { need |= NEED_ROWS; I.need_amount[3] = I.lstart[k] + est; }
-      if (est > I.tent_cap) { need |= NEED_LIST; I.need_amount[2] = est; }
-      if (need) {
-        I.status = ST_NEED_MEM;
-        I.need = need;
-      } else {
-        tiles = t;
-        chunks = (words + kChunkWords - 1) / kChunkWords;
-        tchunks = (cap + kScanSlots - 1) / kScanSlots;
-        I.n_new = I.n_wins = I.probe_fail = I.n_newlist = 0;
-        I.best_cand = I.best_sol = ~0ULL;
-        I.sol_known = 0;
-        I.attempt = (I.attempt_level == k) ? I.attempt + 1 : 1;
-        I.attempt_level = k;
+      plan_one(I);
+      if (I.status == ST_RUNNING) {
+        tiles = I.plan_tiles;
+        chunks = (I.plan_words + kChunkWords - 1) / kChunkWords;
+        tchunks = I.plan_tchunks;
       }
     }
     B.p1_prefix[b + 1] = tiles;
@@ -256,6 +275,7 @@ __device__ void ph_p1(const BatchDev& B) {
 
 __global__ void __launch_bounds__(kTS) k_p1(BatchDev* Bp) {
   const BatchDev B = *Bp;
+  if (blockIdx.x >= B.p1_prefix[B.ninst]) return;   // more CTAs than tiles: no ticket needed
   ph_p1(B);
 }
 
@@ -324,6 +344,66 @@ __device__ void ph_table_scan(const BatchDev& B, unsigned bid, unsigned nb) {
 __global__ void k_table_scan(BatchDev* Bp) {
   const BatchDev B = *Bp;
   ph_table_scan(B, blockIdx.x, gridDim.x);
+}
+
+// Graph solver: k_table_scan, then the last CTA to finish checks every
+// instance's buffers against its owner count (a shortfall asks the host for
+// memory before anything of the level is written) and builds the prefix of
+// row-emission groups (kEmitGroup owners each) over the instances.
+__global__ void k_table_scan_check(BatchDev* Bp) {
+  __shared__ int s_last;
+  __shared__ unsigned long long s_w[32], s_carry;
+  const BatchDev B = *Bp;
+  // CTAs beyond the level's scan chunks (but at least one, and enough warps
+  // for the per-instance settle) leave at once and take no ticket
+  const unsigned long long chunks = B.tscan_prefix[B.ninst];
+  const unsigned long long want = (unsigned long long)(B.ninst + (blockDim.x >> 5) - 1) / (blockDim.x >> 5);
+  unsigned long long part = chunks > want ? chunks : want;
+  if (part > gridDim.x) part = gridDim.x;
+  if (part == 0) part = 1;
+  if (blockIdx.x >= part) return;
+  ph_table_scan(B, blockIdx.x, (unsigned)part);
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s_last = atomicAdd(B.tickets + 1, 1ULL) == part - 1;
+    s_carry = 0;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  for (int base = 0; base < B.ninst; base += blockDim.x) {
+    const int b = base + threadIdx.x;
+    unsigned long long groups = 0;
+    if (b < B.ninst) {
+      InstDev& I = B.inst[b];
+      if (*(volatile int*)&I.status == ST_RUNNING) {
+        const unsigned long long nw = *(volatile unsigned long long*)&I.n_wins;
+        const unsigned long long fails = *(volatile unsigned long long*)&I.probe_fail;
+        const int sk = *(volatile int*)&I.sol_known;
+        const unsigned long long cap = I.table_mask + 1;
+        const int k = I.level;
+        int need = 0;
+        if (fails != 0 || 4 * (I.keys + nw) > 3 * cap) { need |= NEED_TABLE; I.need_amount[1] = 4 * (I.keys + nw) + 4096; }
+        if (nw > I.tent_cap) { need |= NEED_LIST; I.need_amount[2] = nw; }
+        if (!sk && I.lstart[k] + nw > I.row_cap) { need |= NEED_ROWS; I.need_amount[3] = I.lstart[k] + nw; }
+        if (need) {
+          I.need = need;
+          I.planned = 0;
+          I.status = ST_NEED_MEM;
+        } else if (!sk) {
+          groups = (nw + kEmitGroup - 1) / kEmitGroup;
+        }
+      }
+    }
+    unsigned long long tot;
+    const unsigned long long ex = block_excl_scan(groups, s_w, tot);
+    if (b < B.ninst) B.win_prefix[b + 1] = s_carry + ex + groups;
+    __syncthreads();
+    if (threadIdx.x == 0) s_carry += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) B.win_prefix[0] = 0;
 }
 
 // ========================================================== bitmap compaction
@@ -509,33 +589,37 @@ __global__ void k_emit_rows(BatchDev* Bp) {
 }
 
 // ================================================================== finish
+// Bookkeeping of the level just built by a RUNNING instance; on a solution,
+// the formula is rebuilt from the cache (LTL_BS.cu:561-705).
+__device__ void finish_one(InstDev& I) {
+  const int k = I.level;
+  I.keys += I.n_wins;
+  if (I.best_sol != ~0ULL) {
+    const uint64_t g = I.best_sol;
+    uint64_t lo = 0, hi = I.n_wins;   // first index with wins[idx] >= g
+    while (lo < hi) {
+      const uint64_t mid = (lo + hi) >> 1;
+      if (I.wins[mid] < g) lo = mid + 1; else hi = mid;
+    }
+    I.lcount[k] = lo + 1;
+    I.lcands[k] = g + 1;
+    I.sol_index = g;
+    I.res_size = k;
+    I.status = ST_FOUND;
+    reconstruct(I, k, g);
+  } else {
+    I.lcount[k] = I.n_wins;
+    I.lcands[k] = I.cands;
+    I.res_size = k;
+    if (k >= I.max_size) I.status = ST_NOT_FOUND;
+    else I.level = k + 1;
+  }
+}
+
 __device__ void ph_finish(const BatchDev& B, unsigned bid, unsigned nb) {
   for (int b = bid * blockDim.x + threadIdx.x; b < B.ninst; b += nb * blockDim.x) {
     InstDev& I = B.inst[b];
-    if (I.status == ST_RUNNING) {
-      const int k = I.level;
-      I.keys += I.n_wins;
-      if (I.best_sol != ~0ULL) {
-        const uint64_t g = I.best_sol;
-        uint64_t lo = 0, hi = I.n_wins;   // first index with wins[idx] >= g
-        while (lo < hi) {
-          const uint64_t mid = (lo + hi) >> 1;
-          if (I.wins[mid] < g) lo = mid + 1; else hi = mid;
-        }
-        I.lcount[k] = lo + 1;
-        I.lcands[k] = g + 1;
-        I.sol_index = g;
-        I.res_size = k;
-        I.status = ST_FOUND;
-        reconstruct(I, k, g);
-      } else {
-        I.lcount[k] = I.n_wins;
-        I.lcands[k] = I.cands;
-        I.res_size = k;
-        if (k >= I.max_size) I.status = ST_NOT_FOUND;
-        else I.level = k + 1;
-      }
-    }
+    if (I.status == ST_RUNNING) finish_one(I);
     B.status_out[b] = make_int2(I.status, I.need);
   }
 }
@@ -545,24 +629,256 @@ __global__ void k_finish(BatchDev* Bp) {
   ph_finish(B, blockIdx.x, gridDim.x);
 }
 
-__global__ void k_loop_ctl(BatchDev* Bp, cudaGraphConditionalHandle handle, unsigned int max_iter) {
+// ============================================================ level advance
+// One CTA.  built != 0: every RUNNING instance whose level was planned (and
+// so built by the step that just ran) is finished; then every RUNNING
+// instance not yet planned for its current level is planned.  The batch's
+// tile and chunk prefixes are rebuilt from the recorded plans, the
+// look-back states of k_compact cleared and the work tickets reset.
+__global__ void __launch_bounds__(1024) k_advance(BatchDev* Bp, cudaGraphConditionalHandle handle, int built,
+                                                  int loop, unsigned int max_iter) {
   __shared__ int s_run, s_need;
+  __shared__ unsigned long long s_w[32];
+  __shared__ unsigned long long s_carry[3];
   const BatchDev B = *Bp;
-  if (threadIdx.x == 0) { s_run = 0; s_need = 0; }
+  if (threadIdx.x == 0) {
+    s_run = 0;
+    s_need = 0;
+    s_carry[0] = s_carry[1] = s_carry[2] = 0;
+  }
   __syncthreads();
   int run = 0, need = 0;
-  for (int b = threadIdx.x; b < B.ninst; b += blockDim.x) {
-    const int st = B.status_out[b].x;
-    run |= (st == ST_RUNNING);
-    need |= (st == ST_NEED_MEM);
+  for (int base = 0; base < B.ninst; base += blockDim.x) {
+    const int b = base + threadIdx.x;
+    unsigned long long tiles = 0, chunks = 0, tchunks = 0;
+    if (b < B.ninst) {
+      InstDev& I = B.inst[b];
+      if (built && I.status == ST_RUNNING && I.planned == I.level) finish_one(I);
+      if (I.status == ST_RUNNING && I.planned != I.level) plan_one(I);
+      if (I.status == ST_RUNNING) {
+        tiles = I.plan_tiles;
+        chunks = (I.plan_words + kCompactWords - 1) / kCompactWords;
+        tchunks = I.plan_tchunks;
+        run = 1;
+      }
+      need |= (I.status == ST_NEED_MEM);
+      B.status_out[b] = make_int2(I.status, I.need);
+    }
+    // inclusive prefixes over this block of instances, carried across blocks
+    unsigned long long tot;
+    const unsigned long long e0 = block_excl_scan(tiles, s_w, tot);
+    if (b < B.ninst) B.p1_prefix[b + 1] = s_carry[0] + e0 + tiles;
+    __syncthreads();
+    if (threadIdx.x == 0) s_carry[0] += tot;
+    const unsigned long long e1 = block_excl_scan(chunks, s_w, tot);
+    if (b < B.ninst) B.chunk_prefix[b + 1] = s_carry[1] + e1 + chunks;
+    __syncthreads();
+    if (threadIdx.x == 0) s_carry[1] += tot;
+    const unsigned long long e2 = block_excl_scan(tchunks, s_w, tot);
+    if (b < B.ninst) B.tscan_prefix[b + 1] = s_carry[2] + e2 + tchunks;
+    __syncthreads();
+    if (threadIdx.x == 0) s_carry[2] += tot;
+    __syncthreads();
   }
   if (run) atomicOr(&s_run, 1);
   if (need) atomicOr(&s_need, 1);
-  __syncthreads();
   if (threadIdx.x == 0) {
+    B.p1_prefix[0] = 0;
+    B.chunk_prefix[0] = 0;
+    B.tscan_prefix[0] = 0;
+    for (int i = 0; i < 4; ++i) B.tickets[i] = 0;
+  }
+  __syncthreads();
+  const unsigned long long nchunks = s_carry[1];
+  for (unsigned long long c = threadIdx.x; c < nchunks; c += blockDim.x) B.chunk_base[c] = 0;
+  if (loop && threadIdx.x == 0) {
     const unsigned long long it = ++(*B.loop_iter);
     const bool more = s_run && !s_need && it < max_iter;
     cudaGraphSetConditional(handle, more ? 1u : 0u);
+  }
+}
+
+// ========================================================= ordered compaction
+// Owner bitmap -> ascending owner list I.wins, in one pass.  CTAs take chunks
+// of kCompactWords bitmap words in ticket order; each counts its owners,
+// publishes the count (flag 1) and then its inclusive prefix (flag 2) in
+// chunk_base, and finds its exclusive prefix by looking back over the
+// preceding chunks of the instance, a warp at a time (decoupled look-back: a
+// chunk waits for its predecessors' counts, which are published as soon as
+// they are known, never for their prefixes).  Instances that are not RUNNING
+// (the table scan's check asked for memory) are skipped; bitmap words are
+// cleared in every case.
+constexpr unsigned long long kFlagCount = 1ULL << 62, kFlagPrefix = 2ULL << 62;
+constexpr unsigned long long kStateMask = (1ULL << 62) - 1;
+constexpr long long kLookbackCycles = 2000000000LL;   // ~1 s: a predecessor that never publishes
+
+__global__ void __launch_bounds__(kCompactThreads) k_compact(BatchDev* Bp) {
+  __shared__ unsigned long long s_w[32];
+  __shared__ unsigned long long s_c, s_prefix;
+  __shared__ int s_ok;
+  const BatchDev B = *Bp;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned long long total = B.chunk_prefix[B.ninst];
+  if (blockIdx.x >= total) return;   // no chunk for this CTA (small levels)
+  for (;;) {
+    if (threadIdx.x == 0) s_c = atomicAdd(B.tickets + 2, 1ULL);
+    __syncthreads();
+    const unsigned long long c = s_c;
+    if (c >= total) break;
+    const int b = find_owner(B.chunk_prefix, B.ninst, c);
+    InstDev& I = B.inst[b];
+    const unsigned long long c0 = B.chunk_prefix[b];
+    const uint64_t words = (I.cands + 31) / 32;
+    const uint64_t w0 = (c - c0) * kCompactWords;
+    uint32_t v[2];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const uint64_t w = w0 + 2 * threadIdx.x + j;
+      v[j] = (w < words) ? __ldcg(I.bitmap + w) : 0u;
+      if (v[j]) I.bitmap[w] = 0u;
+    }
+    const unsigned long long cnt = __popc(v[0]) + __popc(v[1]);
+    unsigned long long tot;
+    const unsigned long long ex = block_excl_scan(cnt, s_w, tot);
+    if (threadIdx.x == 0) {
+      const int ok = *(volatile int*)&I.status == ST_RUNNING;
+      s_ok = ok;
+      if (ok && c == c0) {
+        atomicExch(B.chunk_base + c, kFlagPrefix | tot);
+        s_prefix = 0;
+      } else if (ok) {
+        atomicExch(B.chunk_base + c, kFlagCount | tot);
+      }
+    }
+    __syncthreads();
+    if (s_ok && c != c0 && warp == 0) {
+      // look back: lane i reads chunk (p - i); the nearest chunk with a
+      // published prefix ends the walk (chunks before the instance's first
+      // count as a prefix of 0)
+      unsigned long long prefix = 0;
+      long long p = (long long)c - 1;
+      bool failed = false;
+      for (;;) {
+        const long long q = p - lane;
+        unsigned long long st = kFlagPrefix;
+        if (q >= (long long)c0) {
+          const long long t0 = clock64();
+          st = *(volatile unsigned long long*)(B.chunk_base + q);
+          while ((st >> 62) == 0) {
+            if (clock64() - t0 > kLookbackCycles) break;
+            st = *(volatile unsigned long long*)(B.chunk_base + q);
+          }
+        }
+        if (__any_sync(0xffffffffu, (st >> 62) == 0)) { failed = true; break; }
+        const unsigned pm = __ballot_sync(0xffffffffu, (st >> 62) == 2);
+        const int stop = pm ? __ffs(pm) - 1 : 31;
+        unsigned long long x = lane <= stop ? (st & kStateMask) : 0ULL;
+        x = warp_sum(x);
+        prefix += __shfl_sync(0xffffffffu, x, 0);
+        if (pm) break;
+        p -= 32;
+      }
+      if (lane == 0) {
+        if (failed) {
+          // a predecessor never published: give up on this instance; the
+          // prefix published here keeps successors' writes inside the list
+          atomicExch(&I.status, (int)ST_ERROR);
+          prefix = 0;
+        }
+        atomicExch(B.chunk_base + c, kFlagPrefix | (prefix + tot));
+        s_prefix = prefix;
+      }
+    }
+    __syncthreads();
+    if (s_ok) {
+      unsigned long long pos = s_prefix + ex;
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        uint32_t bits = v[j];
+        const uint64_t gw = (w0 + 2 * threadIdx.x + j) * 32;
+        while (bits) {
+          const int bit = __ffs(bits) - 1;
+          bits &= bits - 1;
+          I.wins[pos++] = gw + bit;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ================================================================ row emission
+// Graph solver: the owners' rows appended to the level cache in canonical
+// order, solution test (insertInCache LTL_BS.cu:299-329).  Work items are
+// groups of kEmitGroup consecutive owners of one instance (prefix built by
+// k_table_scan_check); a warp takes one group at a time, lane per trace word,
+// so row reads and writes stay coalesced and the loads of every owner of the
+// group are in flight together.
+__global__ void k_emit(BatchDev* Bp) {
+  const BatchDev B = *Bp;
+  const unsigned long long total = B.win_prefix[B.ninst];
+  const int lane = threadIdx.x & 31;
+  const unsigned long long nw = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
+  for (unsigned long long item = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; item < total;
+       item += nw) {
+    const int b = find_owner(B.win_prefix, B.ninst, item);
+    InstDev& I = B.inst[b];
+    if (I.status != ST_RUNNING) continue;
+    const int k = I.level, T = I.T, TP = I.TP;
+    const uint64_t o0 = (item - B.win_prefix[b]) * kEmitGroup;
+    const uint64_t nwin = I.n_wins;
+    // lanes 0..kEmitGroup-1 decode one owner each
+    int op = -1;
+    const uint64_t* pa = nullptr;
+    const uint64_t* pb = nullptr;
+    uint64_t g = 0;
+    if (lane < kEmitGroup && o0 + lane < nwin) {
+      g = __ldcg(I.wins + o0 + lane);
+      const Cand cd = decode(I, k, g);
+      op = cd.op;
+      if (op >= 0) {
+        pa = row_ptr(I, cd.la, cd.a);
+        pb = (op == OP_AND || op == OP_OR || op == OP_U) ? row_ptr(I, cd.lb, cd.b) : pa;
+      }
+    }
+    int ops[kEmitGroup];
+    const uint64_t* ra[kEmitGroup];
+    const uint64_t* rb[kEmitGroup];
+    bool bad[kEmitGroup];
+#pragma unroll
+    for (int u = 0; u < kEmitGroup; ++u) {
+      ops[u] = __shfl_sync(0xffffffffu, op, u);
+      ra[u] = (const uint64_t*)__shfl_sync(0xffffffffu, (unsigned long long)pa, u);
+      rb[u] = (const uint64_t*)__shfl_sync(0xffffffffu, (unsigned long long)pb, u);
+      bad[u] = false;
+    }
+    const uint64_t r0 = I.lstart[k] + o0;
+    for (int t = lane; t < TP; t += 32) {
+      const int L = t < T ? I.len[t] : 0;
+      const uint64_t lab = (t < T && is_pos(I, t)) ? 1ULL : 0ULL;
+      uint64_t xa[kEmitGroup], xb[kEmitGroup];
+#pragma unroll
+      for (int u = 0; u < kEmitGroup; ++u) {
+        xa[u] = (ops[u] >= 0 && t < T) ? __ldg(ra[u] + t) : 0ULL;
+        xb[u] = (ops[u] >= 0 && t < T) ? __ldg(rb[u] + t) : 0ULL;
+      }
+#pragma unroll
+      for (int u = 0; u < kEmitGroup; ++u) {
+        if (ops[u] < 0) continue;
+        const uint64_t word = t < T ? apply_w(ops[u], xa[u], xb[u], L) : 0ULL;
+        if (t < T) bad[u] |= ((word ^ lab) & 1ULL) != 0;
+        I.rows[(r0 + u) * (uint64_t)TP + t] = word;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kEmitGroup; ++u) {
+      if (ops[u] < 0) continue;
+      const bool sol = !__any_sync(0xffffffffu, bad[u]);
+      if (lane == u) {
+        I.origin[r0 + u] = g;
+        if (sol) atomicMin(&I.best_sol, (unsigned long long)g);
+      }
+    }
   }
 }
 

@@ -8,6 +8,9 @@ constexpr int kChunkWords = 4096;     // bitmap words per compaction chunk (1310
 constexpr int kChunkThreads = 256;    // threads per compaction CTA
 constexpr int kScanThreads = 1024;
 constexpr int kScanSlots = 8192;      // hash-set slots per table-scan chunk
+constexpr int kCompactWords = 512;    // owner-bitmap words per k_compact chunk (16384 candidates)
+constexpr int kCompactThreads = 256;  // threads per k_compact CTA (two bitmap words each)
+constexpr int kEmitGroup = 4;         // owners per warp step of k_emit
 
 // Global batch descriptor, resident in device memory so that buffer growth
 // never invalidates a captured launch sequence.
@@ -18,9 +21,11 @@ struct BatchDev {
   unsigned long long* p1_prefix;        // [ninst+1] P1 tiles
   unsigned long long* chunk_prefix;     // [ninst+1] owner-bitmap chunks
   unsigned long long* tscan_prefix;     // [ninst+1] table-scan chunks
-  unsigned long long* win_prefix;       // [ninst+1] owners of new keys
+  unsigned long long* win_prefix;       // [ninst+1] owners of new keys (k_emit_rows), or
+                                        // row-emission groups (k_emit)
   unsigned int* chunk_cnt;              // [chunk_cap]
-  unsigned long long* chunk_base;       // [chunk_cap]
+  unsigned long long* chunk_base;       // [chunk_cap] chunk offsets (k_chunk_*), or the
+                                        // look-back states of k_compact (flag << 62 | count)
   unsigned long long chunk_cap;
   unsigned long long* tickets;          // [4]: P1 work ticket, scan done counter
   int2* status_out;                     // [ninst] (status, need) mirror for the host
@@ -29,7 +34,22 @@ struct BatchDev {
                                         // generation, [2] error, [3] continue flag
 };
 
-// Level-step kernels, launched in this order for every level.
+// Level step of the graph solver: k_p1, k_table_scan_check, k_compact,
+// k_emit, k_advance (k_advance also runs once, with built = 0, before the
+// first step of a launch).  k_table_scan_check adds the buffer checks to the
+// table scan; k_compact replaces k_chunk_count/scan/emit with one ordered
+// pass (decoupled look-back over the chunks); k_advance replaces k_finish +
+// k_plan + the loop control.  With loop != 0 it sets the graph's while
+// condition: some instance RUNNING, none waiting for memory, fewer than
+// max_iter steps.
+__global__ void k_advance(BatchDev* B, cudaGraphConditionalHandle handle, int built, int loop,
+                          unsigned int max_iter);
+__global__ void k_table_scan_check(BatchDev* B);
+__global__ void k_compact(BatchDev* B);
+__global__ void k_emit(BatchDev* B);
+
+// Level-step kernels of the persistent, cluster and allocation-free solvers,
+// launched in this order for every level.
 __global__ void k_plan(BatchDev* B);
 __global__ void k_p1(BatchDev* B);
 __global__ void k_table_scan(BatchDev* B);
@@ -38,9 +58,6 @@ __global__ void k_chunk_scan(BatchDev* B);
 __global__ void k_chunk_emit(BatchDev* B);
 __global__ void k_emit_rows(BatchDev* B);
 __global__ void k_finish(BatchDev* B);
-// Device-side level loop: keeps the graph's while-node running while some
-// instance is RUNNING, none waits for memory and fewer than max_iter steps ran.
-__global__ void k_loop_ctl(BatchDev* B, cudaGraphConditionalHandle handle, unsigned int max_iter);
 
 // Persistent solver: the whole level loop in one cooperative launch (all CTAs
 // co-resident), the phases above separated by a bounded grid barrier.  Runs at

@@ -1,5 +1,5 @@
 // vfb_ops.cuh -- device building blocks shared by the level-step kernels
-// (vfb_kernels.cu) and the persistent solver (vfb_persist.cu): hash-set
+// and the persistent and cluster solvers (vfb_kernels.cu): hash-set
 // insert/find, candidate decoding, key computation, P1 tile processing,
 // scans, formula reconstruction.
 #pragma once
@@ -126,6 +126,23 @@ struct Cand {
   uint64_t a, b;
 };
 
+// q = g / n, r = g % n.  Below 2^52 the quotient comes from one correctly
+// rounded double division (off by at most one, corrected from the remainder),
+// which is much shorter than the 64-bit integer division sequence.
+__device__ __forceinline__ void divmod64(uint64_t g, uint64_t n, uint64_t& q, uint64_t& r) {
+  if (g < (1ULL << 52) && n < (1ULL << 52)) {
+    uint64_t qq = (uint64_t)((double)g / (double)n);
+    long long rr = (long long)(g - qq * n);
+    if (rr < 0) { --qq; rr += (long long)n; }
+    else if ((uint64_t)rr >= n) { ++qq; rr -= (long long)n; }
+    q = qq;
+    r = (uint64_t)rr;
+  } else {
+    q = g / n;
+    r = g % n;
+  }
+}
+
 // Canonical candidate index g of level k -> operator and operands (levels and
 // indices within them).  Block order ~ & | X F G U; & and | over left sizes
 // 1..floor((k-1)/2), U over 1..k-2; left index major (ltl_nocache.cu:169-224).
@@ -143,7 +160,8 @@ __device__ inline Cand decode(const InstDev& I, int k, uint64_t g) {
       const uint64_t cnt = n[i] * n[j];
       if (g < cnt) {
         c.op = pass ? OP_OR : OP_AND;
-        c.la = i; c.lb = j; c.a = g / n[j]; c.b = g % n[j];
+        c.la = i; c.lb = j;
+        divmod64(g, n[j], c.a, c.b);
         return c;
       }
       g -= cnt;
@@ -157,7 +175,8 @@ __device__ inline Cand decode(const InstDev& I, int k, uint64_t g) {
     const int j = k - 1 - i;
     const uint64_t cnt = n[i] * n[j];
     if (g < cnt) {
-      c.op = OP_U; c.la = i; c.lb = j; c.a = g / n[j]; c.b = g % n[j];
+      c.op = OP_U; c.la = i; c.lb = j;
+      divmod64(g, n[j], c.a, c.b);
       return c;
     }
     g -= cnt;
@@ -242,7 +261,7 @@ struct P1Count {
 // bits match every trace's label (a solution candidate).
 template <int N>
 __device__ __forceinline__ void insert_group(InstDev& I, unsigned live, int k, const uint64_t* h,
-                                             const uint64_t* l, const uint64_t* g, const uint64_t* bad,
+                                             const uint64_t* l, const uint64_t* g, const uint32_t* bad,
                                              P1Count& cnt) {
   Slot* tab = I.table;
   const uint64_t mask = I.table_mask;
@@ -285,6 +304,28 @@ __device__ __forceinline__ uint64_t pos_bit(const TileSh& P, int t) {
   return (P.pos[t >> 6] >> (t & 63)) & 1ULL;
 }
 
+// Compile-time half of a trace index: HASH keys fold traces t < T/2 into h,
+// the others into l (LTL_BS.cu:30-110), so the P1 loops run the two halves
+// as separate loops and pick the accumulator statically.
+template <bool HI>
+struct Half {
+  static constexpr bool hi = HI;
+};
+
+template <int MODE, bool HI>
+__device__ __forceinline__ void key_word_h(KeyAcc& k, uint64_t w, int t, int off, int width, int stride, int L) {
+  if (MODE == KEY_HASH) {
+    const uint64_t x = splitmix_fin(w);
+    if (HI) k.a1 ^= x; else k.a0 ^= x;
+  } else {
+    key_word<MODE>(k, w, t, 0, off, width, stride, L);
+  }
+}
+
+// Solution test accumulators: only bit 0 (step 0) of a word is compared
+// with the trace's label, so 32 bits carry the whole test.
+__device__ __forceinline__ uint32_t lo32(uint64_t w) { return (uint32_t)w; }
+
 template <int MODE>
 __device__ inline void p1_unary(InstDev& I, const TileSh& P, const uint64_t* sS, int sp, P1Count& cnt) {
   const uint64_t a = P.s0 + threadIdx.x;
@@ -293,21 +334,25 @@ __device__ inline void p1_unary(InstDev& I, const TileSh& P, const uint64_t* sS,
   const uint64_t* srow = sS + threadIdx.x * sp;
   KeyAcc k0, k1, k2, k3;
   key_init(k0); key_init(k1); key_init(k2); key_init(k3);
-  uint64_t bad[4] = {0, 0, 0, 0};
-  for (int t = 0; t < P.T; ++t) {
+  uint32_t bad[4] = {0, 0, 0, 0};
+  auto body = [&](int t, auto half) {
+    constexpr bool HI = decltype(half)::hi;
     const uint64_t w = srow[t];
     const int L = P.len[t], off = P.off[t], wd = P.wid[t];
-    const uint64_t lm = len_mask(L), pb = pos_bit(P, t);
+    const uint64_t lm = len_mask(L);
+    const uint32_t pb = (uint32_t)pos_bit(P, t);
     const uint64_t w0 = ~w & lm, w1 = w >> 1, w2 = w_fin(w), w3 = w_glob(w, lm);
-    bad[0] |= w0 ^ pb;
-    bad[1] |= w1 ^ pb;
-    bad[2] |= w2 ^ pb;
-    bad[3] |= w3 ^ pb;
-    key_word<MODE>(k0, w0, t, P.half, off, wd, P.stride, L);
-    key_word<MODE>(k1, w1, t, P.half, off, wd, P.stride, L);
-    key_word<MODE>(k2, w2, t, P.half, off, wd, P.stride, L);
-    key_word<MODE>(k3, w3, t, P.half, off, wd, P.stride, L);
-  }
+    bad[0] |= lo32(w0) ^ pb;
+    bad[1] |= lo32(w1) ^ pb;
+    bad[2] |= lo32(w2) ^ pb;
+    bad[3] |= lo32(w3) ^ pb;
+    key_word_h<MODE, HI>(k0, w0, t, off, wd, P.stride, L);
+    key_word_h<MODE, HI>(k1, w1, t, off, wd, P.stride, L);
+    key_word_h<MODE, HI>(k2, w2, t, off, wd, P.stride, L);
+    key_word_h<MODE, HI>(k3, w3, t, off, wd, P.stride, L);
+  };
+  for (int t = 0; t < P.half; ++t) body(t, Half<true>{});
+  for (int t = P.half; t < P.T; ++t) body(t, Half<false>{});
   uint64_t h[4], l[4], g[4];
   key_final<MODE>(k0, h[0], l[0]);
   key_final<MODE>(k1, h[1], l[1]);
@@ -318,7 +363,7 @@ __device__ inline void p1_unary(InstDev& I, const TileSh& P, const uint64_t* sS,
   g[2] = I.base_f + a;
   g[3] = I.base_g + a;
 #pragma unroll
-  for (int j = 0; j < 4; ++j) bad[j] &= 1ULL;
+  for (int j = 0; j < 4; ++j) bad[j] &= 1u;
   insert_group<4>(I, live, P.k, h, l, g, bad, cnt);
 }
 
@@ -334,25 +379,28 @@ __device__ inline void p1_binary(InstDev& I, const TileSh& P, const uint64_t* sS
     const uint64_t* qrow = sQ + q * P.TP;
     KeyAcc kA, kO, kU, kV;
     key_init(kA); key_init(kO); key_init(kU); key_init(kV);
-    uint64_t bad[4] = {0, 0, 0, 0};
-    for (int t = 0; t < P.T; ++t) {
+    uint32_t bad[4] = {0, 0, 0, 0};
+    auto body = [&](int t, auto half) {
+      constexpr bool HI = decltype(half)::hi;
       const uint64_t qw = qrow[t], sw = srow[t];
       const uint64_t la = P.qleft ? qw : sw, lb = P.qleft ? sw : qw;
       const int L = P.len[t], off = P.off[t], wd = P.wid[t];
-      const uint64_t pb = pos_bit(P, t);
+      const uint32_t pb = (uint32_t)pos_bit(P, t);
       const uint64_t wa = la & lb, wo = la | lb, wu = w_until(la, lb);
-      bad[0] |= wa ^ pb;
-      bad[1] |= wo ^ pb;
-      bad[2] |= wu ^ pb;
-      key_word<MODE>(kA, wa, t, P.half, off, wd, P.stride, L);
-      key_word<MODE>(kO, wo, t, P.half, off, wd, P.stride, L);
-      key_word<MODE>(kU, wu, t, P.half, off, wd, P.stride, L);
+      bad[0] |= lo32(wa) ^ pb;
+      bad[1] |= lo32(wo) ^ pb;
+      bad[2] |= lo32(wu) ^ pb;
+      key_word_h<MODE, HI>(kA, wa, t, off, wd, P.stride, L);
+      key_word_h<MODE, HI>(kO, wo, t, off, wd, P.stride, L);
+      key_word_h<MODE, HI>(kU, wu, t, off, wd, P.stride, L);
       if (FOUR) {
         const uint64_t wv = w_until(lb, la);
-        bad[3] |= wv ^ pb;
-        key_word<MODE>(kV, wv, t, P.half, off, wd, P.stride, L);
+        bad[3] |= lo32(wv) ^ pb;
+        key_word_h<MODE, HI>(kV, wv, t, off, wd, P.stride, L);
       }
-    }
+    };
+    for (int t = 0; t < P.half; ++t) body(t, Half<true>{});
+    for (int t = P.half; t < P.T; ++t) body(t, Half<false>{});
     const uint64_t a = P.qleft ? P.q0 + q : s;     // index in level i
     const uint64_t b = P.qleft ? s : P.q0 + q;     // index in level j
     uint64_t h[4], l[4], g[4];
@@ -364,7 +412,7 @@ __device__ inline void p1_binary(InstDev& I, const TileSh& P, const uint64_t* sS
     g[1] = I.base_or[P.i] + ab;
     g[2] = I.base_u[P.i] + ab;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) bad[j] &= 1ULL;
+    for (int j = 0; j < 4; ++j) bad[j] &= 1u;
     if (FOUR) {
       key_final<MODE>(kV, h[3], l[3]);
       g[3] = I.base_u[P.j] + b * P.ni + a;
