@@ -95,6 +95,10 @@ struct InstDev {
   int planned, pad3;             // level the current plan (bases, tiling) was made for; 0: none
   unsigned long long plan_tiles, plan_words, plan_tchunks;   // P1 tiles, bitmap words, table-scan
                                                              // chunks of the current plan
+  // figures of the last level built (for the host's profile): candidates,
+  // owners, hash-set slots the owner scan visited, solution settled early
+  unsigned long long built_cands, built_wins, built_scanned;
+  int built_sol_known, pad4;
   // ---- result
   int res_size, rpn_len;
   int16_t rpn[kMaxSize];

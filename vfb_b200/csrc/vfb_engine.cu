@@ -846,12 +846,16 @@ struct Engine {
       const int j = k - 1 - i;
       operands += (double)(i == j ? n[i] : n[i] + n[j]) * T8;
     }
-    const double cands = (double)d.cands, wins = (double)d.n_wins;
+    // figures of level k as recorded when it was finished
+    const double cands = (double)d.built_cands, wins = (double)d.built_wins;
     const double w0 = std::ceil(cands / 32.0) * 4;
     prof[KP_P1].bytes += operands + 32.0 * cands;
-    prof[KP_TSCAN].bytes += 32.0 * (double)(d.table_mask + 1) + 4.0 * wins;
+    // owner scan: a listed slot costs its list entry and its payload, a full
+    // scan every slot; one bitmap word update per owner
+    const bool listed = d.built_scanned != d.table_mask + 1;
+    prof[KP_TSCAN].bytes += (listed ? 16.0 : 32.0) * (double)d.built_scanned + 4.0 * wins;
     prof[KP_COMPACT].bytes += 2 * w0 + 8.0 * wins;
-    if (!d.sol_known) prof[KP_EMIT].bytes += wins * (2 * T8 + 8.0 * d.TP + 16);
+    if (!d.built_sol_known) prof[KP_EMIT].bytes += wins * (2 * T8 + 8.0 * d.TP + 16);
   }
 
   void profile_step(int n, std::vector<InstHost>& H) {

@@ -593,6 +593,10 @@ __global__ void k_emit_rows(BatchDev* Bp) {
 // the formula is rebuilt from the cache (LTL_BS.cu:561-705).
 __device__ void finish_one(InstDev& I) {
   const int k = I.level;
+  I.built_cands = I.cands;
+  I.built_wins = I.n_wins;
+  I.built_scanned = (I.attempt == 1 && I.n_newlist <= I.tent_cap) ? I.n_newlist : I.table_mask + 1;
+  I.built_sol_known = I.sol_known;
   I.keys += I.n_wins;
   if (I.best_sol != ~0ULL) {
     const uint64_t g = I.best_sol;
