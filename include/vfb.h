@@ -135,16 +135,20 @@ vfb_status vfb_solve_noalloc(const vfb_instance *inst, vfb_result *out);
  * request_bytes finishes with VFB_LIMIT and the sizes it completed.
  * *active / *queued (may be NULL) report the slots in use and the requests
  * waiting.  A request that cannot be admitted finishes with its status.
- * vfb_serve_limits sets budget_frac (default 0.8) and request_bytes (0, the
- * default: a quarter of the budget) for the next vfb_serve_open and the
- * open session. */
+ * A level of more than step_candidates candidates is built over several
+ * steps (slices of its operator tiles), so one large request does not hold
+ * the others' steps for long.  vfb_serve_limits sets budget_frac (default
+ * 0.8), request_bytes (0, the default: a quarter of the budget) and
+ * step_candidates (default 2^25; 0: whole levels) for the next
+ * vfb_serve_open and the open session. */
 typedef struct {
   uint64_t tag;
   vfb_result result;
 } vfb_served;
 
 vfb_status vfb_serve_open(void *ctx, int slots, int max_traces);
-vfb_status vfb_serve_limits(void *ctx, double budget_frac, uint64_t request_bytes);
+vfb_status vfb_serve_limits(void *ctx, double budget_frac, uint64_t request_bytes,
+                            uint64_t step_candidates);
 vfb_status vfb_serve_submit(void *ctx, const vfb_instance *inst, uint64_t tag);
 vfb_status vfb_serve_step(void *ctx, vfb_served *done, int cap, int *ndone, int *active, int *queued);
 void vfb_serve_close(void *ctx);

@@ -73,3 +73,16 @@ def test_tight_budget_still_progresses(engine):
         engine.serve_limits(0.8, 0)
     for (t, prob), got in zip(stream, results):
         assert _key(got) == _key(engine.solve(prob))
+
+
+def test_sliced_levels_equal_solo(engine):
+    # a tiny per-step slice: every level of every request takes many steps
+    insts = [synth.config_planted(), cases.random_instance(4242, 4, 5, 5, 16, 8)] + cases.planted_cases(3)
+    stream = [(0.0, vfb_b200.Problem.from_instance(i)) for i in insts]
+    try:
+        engine.serve_limits(0.8, 0, 2000)
+        results, _, _ = serve.run_stream(engine, stream, slots=4)
+    finally:
+        engine.serve_limits(0.8, 0)
+    for (t, prob), got in zip(stream, results):
+        assert _key(got) == _key(engine.solve(prob))

@@ -117,7 +117,7 @@ def load_library():
     lib.vfb_solve_noalloc.restype = ctypes.c_int
     lib.vfb_serve_open.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     lib.vfb_serve_open.restype = ctypes.c_int
-    lib.vfb_serve_limits.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_uint64]
+    lib.vfb_serve_limits.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_uint64, ctypes.c_uint64]
     lib.vfb_serve_limits.restype = ctypes.c_int
     lib.vfb_serve_submit.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Instance), ctypes.c_uint64]
     lib.vfb_serve_submit.restype = ctypes.c_int
@@ -275,9 +275,11 @@ class Engine:
         return _result(res)
 
     # ---- serving (continuous batching)
-    def serve_limits(self, budget_frac: float = 0.8, request_bytes: int = 0) -> None:
-        """Admission fraction of the memory budget and per-request byte cap (0: budget / 4)."""
-        rc = self._lib.vfb_serve_limits(self._ctx, budget_frac, request_bytes)
+    def serve_limits(self, budget_frac: float = 0.8, request_bytes: int = 0,
+                     step_candidates: int = 1 << 25) -> None:
+        """Admission fraction of the memory budget, per-request byte cap (0: budget / 4) and
+        operator candidates of one request per step (0: whole levels)."""
+        rc = self._lib.vfb_serve_limits(self._ctx, budget_frac, request_bytes, step_candidates)
         if rc != OK:
             raise VfbError(f"vfb_serve_limits failed: {STATUS_NAMES[rc]}")
 

@@ -92,7 +92,11 @@ struct InstDev {
   int sol_known, pad2;           // best_sol settled before the rows were emitted
   unsigned long long n_newlist;  // slots of keys first inserted by this level's P1 (listed in wins)
   int attempt, attempt_level;    // attempts at the current level (> 1: a retry after growth)
-  int planned, pad3;             // level the current plan (bases, tiling) was made for; 0: none
+  int planned, p1_tail;          // level the current plan (bases, tiling) was made for (0: none);
+                                 // 1 when this step's k_p1 finishes the level's tiles
+  unsigned long long p1_done;    // tiles of the level processed by earlier steps
+  unsigned long long p1_step;    // tiles this step processes
+  unsigned long long p1_quota;   // candidates per step (0: the whole level in one step)
   unsigned long long plan_tiles, plan_words, plan_tchunks;   // P1 tiles, bitmap words, table-scan
                                                              // chunks of the current plan
   // figures of the last level built (for the host's profile): candidates,

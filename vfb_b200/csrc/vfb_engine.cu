@@ -59,6 +59,9 @@ const int kStepSeq[] = {KP_ADVANCE, KP_P1, KP_TSCAN, KP_COMPACT, KP_EMIT, KP_ADV
 constexpr int kStepLen = sizeof(kStepSeq) / sizeof(int);
 constexpr int kBodyLen = 5;   // kernels of one level inside the device-side loop
 constexpr unsigned kMaxLoop = 4 * kMaxSize;
+// serving: P1 candidates of one request per step (a larger level takes
+// several steps), which bounds the step that every resident request waits for
+constexpr uint64_t kServeStepCands = 1ull << 25;
 // candidates of one level above which an instance leaves the cluster solver
 constexpr unsigned long long kPromoteAbove = 1ULL << 21;
 
@@ -1114,19 +1117,24 @@ struct Engine {
     int p1_smem = 0;
     double budget_frac = 0.8;     // admission: projected bytes of all slots <= budget_frac * budget
     uint64_t request_bytes = 0;   // per-request cap (0: a quarter of the budget)
+    uint64_t step_cands = 0;      // P1 candidates per request per step (0: whole levels)
   } sv;
 
-  // Admission fraction and per-request byte cap of the serving session.
-  vfb_status serve_limits(double budget_frac, uint64_t request_bytes) {
+  // Admission fraction, per-request byte cap and per-step candidate slice of
+  // the serving session.
+  vfb_status serve_limits(double budget_frac, uint64_t request_bytes, uint64_t step_candidates) {
     if (!(budget_frac > 0.0 && budget_frac <= 1.0)) return VFB_BAD_INPUT;
     sv_budget_frac = budget_frac;
     sv_request_bytes = request_bytes;
+    sv_step_cands = step_candidates;
     sv.budget_frac = budget_frac;
     sv.request_bytes = request_bytes;
+    sv.step_cands = step_candidates;
     return VFB_OK;
   }
   double sv_budget_frac = 0.8;
   uint64_t sv_request_bytes = 0;
+  uint64_t sv_step_cands = kServeStepCands;
 
   vfb_status serve_open(int slots, int max_traces) {
     if (slots <= 0) return VFB_BAD_INPUT;
@@ -1139,6 +1147,7 @@ struct Engine {
     sv.proj.assign(slots, 0);
     sv.budget_frac = sv_budget_frac;
     sv.request_bytes = sv_request_bytes ? sv_request_bytes : (uint64_t)(mem_limit / 4);
+    sv.step_cands = sv_step_cands;
     if (cudaMallocHost(&sv.h_inst, (size_t)slots * sizeof(InstDev)) != cudaSuccess) {
       sv.h_inst = nullptr;
       return VFB_OOM;
@@ -1247,6 +1256,7 @@ struct Engine {
         }
         s = alloc_buffers(H, c.rows, c.slots, c.words, c.tents);
         H.d.promote_above = ~0ULL;
+        H.d.p1_quota = sv.step_cands;
       }
       if (s == VFB_OK) {
         std::vector<InstHost> one(1);
@@ -1420,9 +1430,9 @@ vfb_status vfb_serve_open(void* ctx, int slots, int max_traces) {
   return static_cast<Engine*>(ctx)->serve_open(slots, max_traces);
 }
 
-vfb_status vfb_serve_limits(void* ctx, double budget_frac, uint64_t request_bytes) {
+vfb_status vfb_serve_limits(void* ctx, double budget_frac, uint64_t request_bytes, uint64_t step_candidates) {
   if (!ctx) return VFB_BAD_INPUT;
-  return static_cast<Engine*>(ctx)->serve_limits(budget_frac, request_bytes);
+  return static_cast<Engine*>(ctx)->serve_limits(budget_frac, request_bytes, step_candidates);
 }
 
 vfb_status vfb_serve_submit(void* ctx, const vfb_instance* inst, uint64_t tag) {

@@ -99,6 +99,9 @@ __device__ void plan_one(InstDev& I) {
     I.plan_words = words;
     I.plan_tchunks = (cap + kScanSlots - 1) / kScanSlots;
     I.planned = k;
+    I.p1_done = 0;
+    I.p1_step = t;
+    I.p1_tail = 1;
     I.n_new = I.n_wins = I.probe_fail = I.n_newlist = 0;
     I.best_cand = I.best_sol = ~0ULL;
     I.sol_known = 0;
@@ -159,7 +162,7 @@ __device__ void ph_p1(const BatchDev& B) {
       if (tile < total) {
         const int b = find_owner(B.p1_prefix, B.ninst, tile);
         InstDev& I = B.inst[b];
-        const uint64_t local = tile - B.p1_prefix[b];
+        const uint64_t local = tile - B.p1_prefix[b] + I.p1_done;
         int grp = 0;
         while (grp + 1 < kGroups && I.grp_prefix[grp + 1] <= local) ++grp;
         const int k = I.level;
@@ -323,7 +326,7 @@ __device__ void ph_table_scan(const BatchDev& B, unsigned bid, unsigned nb) {
   const unsigned long long nw = ((unsigned long long)nb * blockDim.x) >> 5;
   for (unsigned long long b = gw; b < (unsigned long long)B.ninst; b += nw) {
     InstDev& I = B.inst[b];
-    if (I.status != ST_RUNNING || I.best_cand == ~0ULL) continue;
+    if (I.status != ST_RUNNING || I.best_cand == ~0ULL || !I.p1_tail) continue;
     const int k = I.level;
     const uint64_t g = I.best_cand;
     const Cand cd = decode(I, k, g);
@@ -657,12 +660,26 @@ __global__ void __launch_bounds__(1024) k_advance(BatchDev* Bp, cudaGraphConditi
     unsigned long long tiles = 0, chunks = 0, tchunks = 0;
     if (b < B.ninst) {
       InstDev& I = B.inst[b];
-      if (built && I.status == ST_RUNNING && I.planned == I.level) finish_one(I);
+      if (built && I.status == ST_RUNNING && I.planned == I.level) {
+        if (I.p1_tail) finish_one(I);
+        else I.p1_done += I.p1_step;   // a slice of the level's tiles ran
+      }
       if (I.status == ST_RUNNING && I.planned != I.level) plan_one(I);
       if (I.status == ST_RUNNING) {
-        tiles = I.plan_tiles;
-        chunks = (I.plan_words + kCompactWords - 1) / kCompactWords;
-        tchunks = I.plan_tchunks;
+        // this step's slice of P1 tiles: all that remain, or the quota's worth
+        const unsigned long long left = I.plan_tiles - I.p1_done;
+        unsigned long long step = left;
+        if (I.p1_quota && I.cands > I.p1_quota) {
+          const unsigned long long q = I.p1_quota * I.plan_tiles / I.cands;
+          step = q < 1 ? 1 : (q < left ? q : left);
+        }
+        I.p1_step = step;
+        I.p1_tail = step == left;
+        tiles = step;
+        if (I.p1_tail) {
+          chunks = (I.plan_words + kCompactWords - 1) / kCompactWords;
+          tchunks = I.plan_tchunks;
+        }
         run = 1;
       }
       need |= (I.status == ST_NEED_MEM);

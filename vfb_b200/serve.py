@@ -93,10 +93,12 @@ def main():
     ap.add_argument("--seed", type=int, default=4)
     ap.add_argument("--large-frac", type=float, default=0.05)
     ap.add_argument("--request-gb", type=float, default=0.0, help="per-request cap (0: budget / 4)")
+    ap.add_argument("--step-cands", type=int, default=1 << 25,
+                    help="operator candidates of one request per step (0: whole levels)")
     args = ap.parse_args()
     rates = [float(x) for x in args.rates.split(",")] if args.rates else [args.rate]
     eng = Engine()
-    eng.serve_limits(0.8, int(args.request_gb * (1 << 30)))
+    eng.serve_limits(0.8, int(args.request_gb * (1 << 30)), args.step_cands)
     for rate in rates:
         count = args.count if not args.rates else min(args.count, max(50, int(args.window * rate)))
         stream = request_stream(args.seed, count, rate, args.large_frac)
