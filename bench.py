@@ -12,6 +12,9 @@ e2e     the same metric through the public C ABI (vfb_solve with host buffers,
 roofline  the dominant kernel of a profiling pass over the same steps (CUDA
         events around every launch on the engine's stream), algorithmic bytes
         per launch over its mean duration, against the measured HBM copy peak.
+candidates_per_s  operator candidates evaluated (the per-level candidate
+        counts up to the solution, as the reference's CheckedLTLs) per second
+        of device time.
 cpu_baseline  the CPU restatement (single thread) on a bounded sample.
 --impl reference  the CPU restatement with OpenMP on every host core, same
         workload and metric (the reference itself is CUDA-only).
@@ -271,7 +274,7 @@ def main():
         assert r.status == vfb_b200.OK, r
     torch.cuda.synchronize()
 
-    dev_s, wall_s, units, launches, h2d, d2h = [], [], 0, 0, 0, 0
+    dev_s, wall_s, units, launches, h2d, d2h, cands = [], [], 0, 0, 0, 0, 0
     _barrier(world)
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
@@ -283,6 +286,7 @@ def main():
             wall_s.append(time.perf_counter() - t0)
             dev_s.append(r.device_seconds)
             units += r.total_rows
+            cands += sum(r.level_cands)
             launches += r.kernel_launches
             h2d += r.h2d_bytes
             d2h += r.d2h_bytes
@@ -334,6 +338,7 @@ def main():
         "config": {"workload": WORKLOAD, "parallelism": f"replicas{world}",
                    "l2": "flushed before every step (256 MB write)"},
         "time_to_formula_ms": 1e3 * statistics.median(wall_s),
+        "candidates_per_s": world * cands / dev_total,
         "time_to_formula_device_ms": 1e3 * statistics.median(dev_s),
         "formula": answer,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d // args.steps,

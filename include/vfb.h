@@ -100,6 +100,16 @@ vfb_status vfb_solve(void *ctx, const vfb_instance *inst, vfb_result *out);
 /* Solves n independent instances together; out[i] equals vfb_solve(inst[i]). */
 vfb_status vfb_batch_solve(void *ctx, const vfb_instance *inst, int n, vfb_result *out);
 
+/* Cache-free search, replacing string LTL(...) of ltl_nocache.cu:319-446:
+ * every formula of each size is evaluated in the numbering order of
+ * numberToFormula (ltl_nocache.cu:169-224) with no cache and no
+ * deduplication, and the first solution of that order is returned (the
+ * reference returns a solution of the same size and root operator block;
+ * which one within the block is a race there).  level_cands[k] counts the
+ * formulas evaluated of size k; level_rows stays 0.  Sizes whose formula
+ * count exceeds 2^62 are not searched (VFB_LIMIT). */
+vfb_status vfb_solve_exhaustive(void *ctx, const vfb_instance *inst, vfb_result *out);
+
 /* Solve without allocating.  No counterpart in the reference.
  *
  * For callers that may not allocate device (or pinned host) memory while they

@@ -73,7 +73,8 @@ class _JsonProblem(ctypes.Structure):
 EXPORTS = ["vfb_create", "vfb_destroy", "vfb_solve", "vfb_batch_solve", "vfb_status_str",
            "vfb_read_json", "vfb_json_free", "vfb_format_infix", "vfb_profile_read",
            "vfb_profile_reset", "vfb_solve_noalloc", "vfb_synth_planted", "vfb_serve_open",
-           "vfb_serve_limits", "vfb_serve_submit", "vfb_serve_step", "vfb_serve_close"]
+           "vfb_serve_limits", "vfb_serve_submit", "vfb_serve_step", "vfb_serve_close",
+           "vfb_solve_exhaustive"]
 
 _lib = None
 
@@ -117,6 +118,8 @@ def load_library():
     lib.vfb_solve_noalloc.restype = ctypes.c_int
     lib.vfb_serve_open.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     lib.vfb_serve_open.restype = ctypes.c_int
+    lib.vfb_solve_exhaustive.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Instance), ctypes.POINTER(_Result)]
+    lib.vfb_solve_exhaustive.restype = ctypes.c_int
     lib.vfb_serve_limits.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_uint64, ctypes.c_uint64]
     lib.vfb_serve_limits.restype = ctypes.c_int
     lib.vfb_serve_submit.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Instance), ctypes.c_uint64]
@@ -271,6 +274,14 @@ class Engine:
         inst, keep = prob._cstruct()
         res = _Result()
         self._lib.vfb_solve(self._ctx, ctypes.byref(inst), ctypes.byref(res))
+        del keep
+        return _result(res)
+
+    def solve_exhaustive(self, prob: Problem) -> Result:
+        """Cache-free search in formula-number order (the ltl_nocache method)."""
+        inst, keep = prob._cstruct()
+        res = _Result()
+        self._lib.vfb_solve_exhaustive(self._ctx, ctypes.byref(inst), ctypes.byref(res))
         del keep
         return _result(res)
 

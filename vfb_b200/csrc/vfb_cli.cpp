@@ -11,6 +11,8 @@
 //   --stats        per-size unique/candidate counts as one JSON line on stderr
 //   --quiet        no progress lines
 //   --strict-exit  non-zero exit status on errors and when nothing is found
+//   --nocache      cache-free search in formula-number order (the reference's
+//                  ltl_nocache method) instead of the cached search
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -28,7 +30,7 @@ static void usage(const char* prog) {
 
 int main(int argc, char** argv) {
   std::vector<const char*> pos;
-  int rlx = 3, device = 0, stats = 0, quiet = 0, strict = 0;
+  int rlx = 3, device = 0, stats = 0, quiet = 0, strict = 0, nocache = 0;
   double mem_gb = 0;
   for (int i = 1; i < argc; ++i) {
     const std::string a = argv[i];
@@ -38,6 +40,7 @@ int main(int argc, char** argv) {
     else if (a == "--stats") stats = 1;
     else if (a == "--quiet") quiet = 1;
     else if (a == "--strict-exit") strict = 1;
+    else if (a == "--nocache") nocache = 1;
     else pos.push_back(argv[i]);
   }
   if (pos.size() != 2) {
@@ -96,7 +99,7 @@ int main(int argc, char** argv) {
   inst.max_size = maxLen;
   inst.rlx_type = rlx;
   vfb_result res;
-  s = vfb_solve(ctx, &inst, &res);
+  s = nocache ? vfb_solve_exhaustive(ctx, &inst, &res) : vfb_solve(ctx, &inst, &res);
   int rc = 0;
   if (res.status == VFB_OK) {
     const int n = vfb_format_infix(&res, jp->names, nullptr, 0);

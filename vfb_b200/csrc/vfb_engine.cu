@@ -1363,6 +1363,138 @@ struct Engine {
     return VFB_OK;
   }
 
+  // ============================================================ cache-free search
+  // Formula numbers of each size in order (ltl_nocache.cu:319-446), one launch
+  // per range of kExhRange numbers; the first range with a solution gives the
+  // first solution of the numbering.  Sizes whose count passes 2^62 end the
+  // search with VFB_LIMIT.
+  static constexpr unsigned long long kExhRange = 1ull << 28;
+
+  static void exh_decode_host(uint64_t n, int k, const uint64_t (*cnt)[8], int16_t* rpn) {
+    if (k == 1) { rpn[0] = (int16_t)n; return; }
+    int op = 0;
+    while (op < OP_U && n >= cnt[k][op]) n -= cnt[k][op++];
+    rpn[k - 1] = (int16_t)(-(1 + op));
+    const int sub = k - 1;
+    if (op == OP_NOT || op == OP_X || op == OP_F || op == OP_G) {
+      exh_decode_host(n, sub, cnt, rpn);
+      return;
+    }
+    int left = 1;
+    while (left < sub - 1 && n >= cnt[left][7] * cnt[sub - left][7]) {
+      n -= cnt[left][7] * cnt[sub - left][7];
+      ++left;
+    }
+    const uint64_t nr = cnt[sub - left][7];
+    exh_decode_host(n / nr, left, cnt, rpn);
+    exh_decode_host(n % nr, sub - left, cnt, rpn + left);
+  }
+
+  vfb_status exhaustive(const vfb_instance& in, vfb_result& r) {
+    const auto t0 = std::chrono::steady_clock::now();
+    std::memset(&r, 0, sizeof(r));
+    c_h2d = c_d2h = c_launch = 0;
+    if (cudaSetDevice(device) != cudaSuccess) return r.status = dev_fail(__LINE__);
+    const int T = in.num_traces, A = in.num_vars, K = in.max_size;
+    if (T < 1 || T > kMaxTraces || A < 1 || A > VFB_MAX_VARS || in.num_pos < 0 || in.num_pos > T ||
+        K < 1 || K > kMaxSize)
+      return r.status = VFB_LIMIT;
+    if (!in.words || !in.lengths) return r.status = VFB_BAD_INPUT;
+    std::vector<ExhDev> hv(1);
+    ExhDev& h = hv[0];
+    std::memset(&h, 0, sizeof(h));
+    h.A = A;
+    h.T = T;
+    for (int t = 0; t < T; ++t) {
+      if (in.lengths[t] < 1 || in.lengths[t] > VFB_MAX_LENGTH) return r.status = VFB_LIMIT;
+      h.len[t] = (uint8_t)in.lengths[t];
+      if (t < in.num_pos) h.posmask[t >> 6] |= 1ULL << (t & 63);
+      const uint64_t m = in.lengths[t] >= 64 ? ~0ULL : ((1ULL << in.lengths[t]) - 1);
+      for (int v = 0; v < A; ++v) h.words[(size_t)t * A + v] = in.words[(size_t)t * A + v] & m;
+    }
+    // count matrix (generateMatrix ltl_nocache.cu:248-287) in 128 bits; the
+    // search stops before the first size that does not fit 62 bits
+    typedef unsigned __int128 u128;
+    u128 c[kMaxSize + 1][8];
+    std::memset(c, 0, sizeof(c));
+    c[1][7] = (u128)A;
+    if (K >= 2) { c[2][0] = c[2][3] = c[2][4] = c[2][5] = (u128)A; c[2][7] = 4 * (u128)A; }
+    for (int i = 3; i <= K; ++i) {
+      u128 un = c[i - 1][7], com = 0, ncom = 0;
+      for (int j = 1; j <= (i - 1) / 2; ++j) com += c[j][7] * c[i - j - 1][7];
+      for (int j = 1; j <= i - 2; ++j) ncom += c[j][7] * c[i - j - 1][7];
+      c[i][0] = c[i][3] = c[i][4] = c[i][5] = un;
+      c[i][1] = c[i][2] = com;
+      c[i][6] = ncom;
+      c[i][7] = 4 * un + 2 * com + ncom;
+    }
+    int kfit = 0;
+    for (int i = 1; i <= K; ++i) {
+      if (c[i][7] >= ((u128)1 << 62)) break;
+      kfit = i;
+    }
+    for (int i = 1; i <= kfit; ++i)
+      for (int o = 0; o < 8; ++o) h.cnt[i][o] = (uint64_t)c[i][o];
+    size_t g1 = 0, g2 = 0;
+    void* pd = dalloc(sizeof(ExhDev), &g1);
+    void* pb = pd ? dalloc(sizeof(unsigned long long), &g2) : nullptr;
+    if (!pd || !pb) { dfree(pd); return r.status = VFB_OOM; }
+    ExhDev* dP = (ExhDev*)pd;
+    unsigned long long* dBest = (unsigned long long*)pb;
+    cudaEventRecord(ev_t0, stream);
+    vfb_status rc = VFB_OK;
+    if (cudaMemcpyAsync(dP, &h, sizeof(ExhDev), cudaMemcpyHostToDevice, stream) != cudaSuccess ||
+        cudaMemsetAsync(dBest, 0xFF, sizeof(unsigned long long), stream) != cudaSuccess)
+      rc = dev_fail(__LINE__);
+    c_h2d += sizeof(ExhDev);
+    unsigned long long best = ~0ULL;
+    int found_k = 0;
+    for (int k = 1; k <= kfit && rc == VFB_OK && !found_k; ++k) {
+      const unsigned long long total = h.cnt[k][7];
+      for (unsigned long long lo = 0; lo < total; lo += kExhRange) {
+        const unsigned long long hi = std::min(total, lo + kExhRange);
+        const unsigned long long nthreads = hi - lo;
+        const unsigned blocks = (unsigned)std::min<unsigned long long>((nthreads + 255) / 256,
+                                                                       (unsigned long long)sms * 16);
+        k_exhaustive<<<blocks, 256, 0, stream>>>(dP, k, lo, hi, dBest);
+        ++c_launch;
+        if (cudaMemcpyAsync(&best, dBest, sizeof(best), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+            cudaStreamSynchronize(stream) != cudaSuccess) {
+          rc = dev_fail(__LINE__);
+          break;
+        }
+        c_d2h += sizeof(best);
+        if (best != ~0ULL) {
+          r.level_cands[k] = best + 1;
+          found_k = k;
+          break;
+        }
+        r.level_cands[k] = hi;
+      }
+      r.size = k;
+    }
+    cudaEventRecord(ev_t1, stream);
+    cudaStreamSynchronize(stream);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev_t0, ev_t1);
+    dfree(pd);
+    dfree(pb);
+    if (rc != VFB_OK) return r.status = rc;
+    r.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    r.device_seconds = ms * 1e-3;
+    r.h2d_bytes = c_h2d;
+    r.d2h_bytes = c_d2h;
+    r.kernel_launches = c_launch;
+    if (found_k) {
+      exh_decode_host(best, found_k, h.cnt, r.rpn);
+      r.rpn_len = found_k;
+      r.solution_index = best;
+      r.size = found_k;
+      return r.status = VFB_OK;
+    }
+    return r.status = (kfit < K) ? VFB_LIMIT : VFB_NOT_FOUND;
+  }
+
   int profile_read(vfb_kernel_stat* outp, int cap) {
     int m = 0;
     for (int k = 0; k < KP_N && m < cap; ++k) {
@@ -1418,6 +1550,11 @@ vfb_status vfb_solve(void* ctx, const vfb_instance* inst, vfb_result* out) {
   if (!ctx || !inst || !out) return VFB_BAD_INPUT;
   const vfb_status rc = static_cast<Engine*>(ctx)->batch(inst, 1, out);
   return rc != VFB_OK ? rc : out->status;
+}
+
+vfb_status vfb_solve_exhaustive(void* ctx, const vfb_instance* inst, vfb_result* out) {
+  if (!ctx || !inst || !out) return VFB_BAD_INPUT;
+  return static_cast<Engine*>(ctx)->exhaustive(*inst, *out);
 }
 
 vfb_status vfb_batch_solve(void* ctx, const vfb_instance* inst, int n, vfb_result* out) {

@@ -77,6 +77,19 @@ struct ClusterWork {
 };
 __global__ void k_cluster(ClusterWork W);
 
+// Cache-free search (vfb_exhaustive.cu): the instance and the count matrix
+// of the formula numbering; formula numbers [lo, hi) of size k are evaluated
+// and the smallest solving number lowers *best.
+struct ExhDev {
+  int A, T;
+  uint64_t cnt[kMaxSize + 1][8];   // formulas per size and root operator (7: all of the size)
+  uint64_t posmask[2];             // bit t: trace t is positive
+  uint8_t len[kMaxTraces];
+  uint64_t words[kMaxTraces * 64]; // words[t * A + v]: proposition v on trace t
+};
+__global__ void k_exhaustive(const ExhDev* P, int k, unsigned long long lo, unsigned long long hi,
+                             unsigned long long* best);
+
 // Set-up and maintenance kernels.
 __global__ void k_init(BatchDev* B);
 __global__ void k_rehash(const Slot* old_tab, unsigned long long old_cap, Slot* new_tab,
