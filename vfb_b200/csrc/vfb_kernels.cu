@@ -156,52 +156,66 @@ __device__ void ph_p1(const BatchDev& B) {
   __shared__ unsigned long long s_red[3][kTS / 32];
   const unsigned long long total = B.p1_prefix[B.ninst];
   while (true) {
-    if (threadIdx.x == 0) {
-      const unsigned long long tile = atomicAdd(B.tickets, 1ULL);
-      P.tile = tile;
+    if (threadIdx.x < 32) {
+      // tile set-up by warp 0: the group boundaries are read one per lane and
+      // the remaining fields with their loads issued before any shared store,
+      // so the chain is a few memory round trips long
+      const int lane = threadIdx.x;
+      unsigned long long tile = 0;
+      if (lane == 0) tile = atomicAdd(B.tickets, 1ULL);
+      tile = __shfl_sync(0xffffffffu, tile, 0);
+      if (lane == 0) P.tile = tile;
       if (tile < total) {
         const int b = find_owner(B.p1_prefix, B.ninst, tile);
-        InstDev& I = B.inst[b];
-        const uint64_t local = tile - B.p1_prefix[b] + I.p1_done;
-        int grp = 0;
-        while (grp + 1 < kGroups && I.grp_prefix[grp + 1] <= local) ++grp;
-        const int k = I.level;
-        P.inst = b;
-        P.grp = grp;
-        P.k = k;
-        P.T = I.T;
-        P.TP = I.TP;
-        P.half = I.T / 2;
-        P.stride = I.stride1;
-        P.mode = I.key_mode;
-        P.tq = I.tq;
-        P.pos[0] = I.posmask[0];
-        P.pos[1] = I.posmask[1];
-        // give up early once the table is known to be too small for this level
-        const unsigned long long cap = I.table_mask + 1;
-        P.skip = (*(volatile unsigned long long*)&I.probe_fail != 0) ||
-                 (4 * (I.keys + *(volatile unsigned long long*)&I.n_new) > 3 * cap);
-        const uint64_t within = local - I.grp_prefix[grp];
-        if (grp == 0) {
-          P.si = k - 1;
-          P.nS = I.lcount[k - 1];
-          P.s0 = within * kTS;
-        } else {
-          const int i = grp, j = k - 1 - i;
-          const uint64_t ni = I.lcount[i], nj = I.lcount[j];
-          const int qleft = (i == j) || (ni <= nj);
-          P.i = i;
-          P.j = j;
-          P.ni = ni;
-          P.nj = nj;
-          P.qleft = qleft;
-          P.si = qleft ? j : i;
-          P.qi = qleft ? i : j;
-          P.nS = qleft ? nj : ni;
-          P.nQ = qleft ? ni : nj;
-          const uint64_t qt = I.grp_qtiles[grp];
-          P.s0 = (within / qt) * kTS;
-          P.q0 = (within % qt) * I.tq;
+        const InstDev* Ip = B.inst + b;
+        const uint64_t local = tile - B.p1_prefix[b] + __ldcg(&Ip->p1_done);
+        const uint64_t gpl = (lane >= 1 && lane < kGroups) ? __ldcg(&Ip->grp_prefix[lane]) : ~0ULL;
+        const int grp = __popc(__ballot_sync(0xffffffffu, gpl <= local));
+        const uint64_t gstart = __shfl_sync(0xffffffffu, gpl, grp);
+        if (lane == 0) {
+          const int k = __ldcg(&Ip->level), T = __ldcg(&Ip->T), TP = __ldcg(&Ip->TP);
+          const int stride = __ldcg(&Ip->stride1), mode = __ldcg(&Ip->key_mode), tq = __ldcg(&Ip->tq);
+          const uint64_t pos0 = __ldcg(&Ip->posmask[0]), pos1 = __ldcg(&Ip->posmask[1]);
+          const unsigned long long cap = __ldcg(&Ip->table_mask) + 1, keys = __ldcg(&Ip->keys);
+          const unsigned long long fails = __ldcg(&Ip->probe_fail), fresh = __ldcg(&Ip->n_new);
+          const int i = grp, j = k - 1 - grp;
+          const uint64_t nk1 = __ldcg(&Ip->lcount[k - 1]);
+          const uint64_t ni = grp ? __ldcg(&Ip->lcount[i]) : 0, nj = grp ? __ldcg(&Ip->lcount[j]) : 0;
+          const uint64_t qt = grp ? __ldcg(&Ip->grp_qtiles[grp]) : 1;
+          const uint64_t within = local - (grp ? gstart : 0);
+          P.inst = b;
+          P.grp = grp;
+          P.k = k;
+          P.T = T;
+          P.TP = TP;
+          P.half = T / 2;
+          P.stride = stride;
+          P.mode = mode;
+          P.tq = tq;
+          P.pos[0] = pos0;
+          P.pos[1] = pos1;
+          // give up early once the table is known to be too small for this level
+          P.skip = (fails != 0) || (4 * (keys + fresh) > 3 * cap);
+          if (grp == 0) {
+            P.si = k - 1;
+            P.nS = nk1;
+            P.s0 = within * kTS;
+          } else {
+            const int qleft = (i == j) || (ni <= nj);
+            P.i = i;
+            P.j = j;
+            P.ni = ni;
+            P.nj = nj;
+            P.qleft = qleft;
+            P.si = qleft ? j : i;
+            P.qi = qleft ? i : j;
+            P.nS = qleft ? nj : ni;
+            P.nQ = qleft ? ni : nj;
+            uint64_t sq, qr;
+            divmod64(within, qt, sq, qr);
+            P.s0 = sq * kTS;
+            P.q0 = qr * tq;
+          }
         }
       }
     }
@@ -224,6 +238,7 @@ __device__ void ph_p1(const BatchDev& B) {
         const int nq = (int)((P.nQ - P.q0) < (uint64_t)P.tq ? (P.nQ - P.q0) : (uint64_t)P.tq);
         stage_rows(sQ, P.TP, row_ptr(I, P.qi, P.q0), nq, P.TP);
       }
+      stage_wait();
     }
     __syncthreads();
     if (!P.skip) {

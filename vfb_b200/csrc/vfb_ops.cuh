@@ -239,18 +239,24 @@ struct TileSh {
   uint8_t len[kMaxTraces], off[kMaxTraces], wid[kMaxTraces];
 };
 
-// Copy nrows consecutive rows (pitch TP words, 16-byte aligned) into shared
-// memory with pitch sp, as 128-bit coalesced loads.
+// Copy nrows consecutive rows (pitch TP words) into shared memory with pitch
+// sp, one 8-byte asynchronous copy per word (cp.async: no registers held, every
+// copy of the tile in flight at once); stage_wait() completes them.  Rows
+// with an odd pitch are only 8-byte aligned, hence 8-byte copies.
 __device__ __forceinline__ void stage_rows(uint64_t* dst, int sp, const uint64_t* src, int nrows, int TP) {
-  const int n2 = nrows * TP / 2;
-  const ulonglong2* s2 = reinterpret_cast<const ulonglong2*>(src);
-  for (int u = threadIdx.x; u < n2; u += blockDim.x) {
-    const ulonglong2 v = __ldcg(s2 + u);
-    const int w = 2 * u, r = w / TP, c = w - r * TP;
-    dst[r * sp + c] = v.x;
-    dst[r * sp + c + 1] = v.y;
+  const int n = nrows * TP;
+  const int dr = blockDim.x / TP, dc = blockDim.x - dr * TP;
+  int r = threadIdx.x / TP, c = threadIdx.x - r * TP;
+  for (int w = threadIdx.x; w < n; w += blockDim.x) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst + r * sp + c);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(src + w) : "memory");
+    r += dr;
+    c += dc;
+    if (c >= TP) { c -= TP; ++r; }
   }
 }
+
+__device__ __forceinline__ void stage_wait() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 struct P1Count {
   unsigned long long fresh, fail, sol;   // keys inserted, probe failures, min solution candidate
