@@ -334,24 +334,46 @@ struct Engine {
   // --------------------------------------------------------- step launch
   // pre: the leading k_advance (plans instances coming from k_init or a
   // growth).  loop: the trailing k_advance sets the while-node's condition.
+  // Launch of one kernel of the step; with pdl, as a programmatic dependent of
+  // the kernel before it on the stream (the kernels wait for it on entry).
+  template <typename... Args>
+  void step_launch(bool pdl, void (*kern)(Args...), unsigned grid_x, unsigned block_x, size_t smem,
+                   Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid_x);
+    cfg.blockDim = dim3(block_x);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kern, args...);
+  }
+
   void launch_step(bool pre, bool timed, int p1_smem, cudaGraphConditionalHandle handle, bool loop) {
     int e = 0;
-    // external event nodes keep their timestamps inside a captured graph
+    // external event nodes keep their timestamps inside a captured graph;
+    // between them the kernels are not adjacent, so no programmatic launch
     auto mark = [&]() { if (timed) cudaEventRecordWithFlags(ev_k[e++], stream, cudaEventRecordExternal); };
+    const bool pdl = !timed;
+    const int lp = loop ? 1 : 0, built0 = 0, built1 = 1;
+    unsigned int mx = kMaxLoop;
     mark();
     if (pre) {
-      k_advance<<<1, adv_threads, 0, stream>>>(dB, handle, 0, loop ? 1 : 0, kMaxLoop);
+      step_launch(false, k_advance, 1u, (unsigned)adv_threads, 0, dB, handle, built0, lp, mx);
       mark();
     }
-    k_p1<<<p1_grid, kTS, p1_smem, stream>>>(dB);
+    step_launch(pdl && pre, k_p1, (unsigned)p1_grid, (unsigned)kTS, (size_t)p1_smem, dB);
     mark();
-    k_table_scan_check<<<grid, 256, 0, stream>>>(dB);
+    step_launch(pdl, k_table_scan_check, (unsigned)grid, 256u, 0, dB);
     mark();
-    k_compact<<<sms * 8, kCompactThreads, 0, stream>>>(dB);
+    step_launch(pdl, k_compact, (unsigned)(sms * 8), (unsigned)kCompactThreads, 0, dB);
     mark();
-    k_emit<<<grid, 256, 0, stream>>>(dB);
+    step_launch(pdl, k_emit, (unsigned)grid, 256u, 0, dB);
     mark();
-    k_advance<<<1, adv_threads, 0, stream>>>(dB, handle, 1, loop ? 1 : 0, kMaxLoop);
+    step_launch(pdl, k_advance, 1u, (unsigned)adv_threads, 0, dB, handle, built1, lp, mx);
     mark();
   }
 

@@ -35,6 +35,15 @@
 
 namespace vfb {
 
+// Programmatic dependent launch inside the level step: wait until the
+// preceding kernel has completed and its writes are visible, then let the
+// next kernel be scheduled while this one runs (its CTAs then wait here
+// themselves).  Both are no-ops for a launch without the attribute.
+__device__ __forceinline__ void step_entry() {
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
 // ===================================================================== plan
 // Plan level k = I.level of a RUNNING instance: candidate-block bases, P1
 // tiling, buffer checks.  Records the plan (planned = k, plan_*) or asks the
@@ -292,6 +301,7 @@ __device__ void ph_p1(const BatchDev& B) {
 }
 
 __global__ void __launch_bounds__(kTS) k_p1(BatchDev* Bp) {
+  step_entry();
   const BatchDev B = *Bp;
   if (blockIdx.x >= B.p1_prefix[B.ninst]) return;   // more CTAs than tiles: no ticket needed
   ph_p1(B);
@@ -371,6 +381,7 @@ __global__ void k_table_scan(BatchDev* Bp) {
 __global__ void k_table_scan_check(BatchDev* Bp) {
   __shared__ int s_last;
   __shared__ unsigned long long s_w[32], s_carry;
+  step_entry();
   const BatchDev B = *Bp;
   // CTAs beyond the level's scan chunks (but at least one, and enough warps
   // for the per-instance settle) leave at once and take no ticket
@@ -662,6 +673,7 @@ __global__ void __launch_bounds__(1024) k_advance(BatchDev* Bp, cudaGraphConditi
   __shared__ int s_run, s_need;
   __shared__ unsigned long long s_w[32];
   __shared__ unsigned long long s_carry[3];
+  step_entry();
   const BatchDev B = *Bp;
   if (threadIdx.x == 0) {
     s_run = 0;
@@ -752,6 +764,7 @@ __global__ void __launch_bounds__(kCompactThreads) k_compact(BatchDev* Bp) {
   __shared__ unsigned long long s_w[32];
   __shared__ unsigned long long s_c, s_prefix;
   __shared__ int s_ok;
+  step_entry();
   const BatchDev B = *Bp;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned long long total = B.chunk_prefix[B.ninst];
@@ -851,6 +864,7 @@ __global__ void __launch_bounds__(kCompactThreads) k_compact(BatchDev* Bp) {
 // so row reads and writes stay coalesced and the loads of every owner of the
 // group are in flight together.
 __global__ void k_emit(BatchDev* Bp) {
+  step_entry();
   const BatchDev B = *Bp;
   const unsigned long long total = B.win_prefix[B.ninst];
   const int lane = threadIdx.x & 31;
