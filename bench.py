@@ -217,10 +217,16 @@ def large_roofline(local: int, peak: float):
     eng.close()
     name, nl, ms, nbytes = max(prof, key=lambda q: q[2])
     achieved = nbytes / (ms * 1e-3) / 1e9
+    per = {}
+    for q in prof:
+        rate = q[3] / (q[2] * 1e-3) / 1e9 if q[2] > 0 and q[3] > 0 else None
+        per[q[0]] = {"ms": round(q[2], 3), "launches": q[1],
+                     "algorithmic_gbs": round(rate, 1) if rate else None,
+                     "frac": round(rate / peak, 4) if rate else None}
     return {"instance": "mixed batch #2 (7 APs, 36 traces, size 9, 11.3M unique CS)",
             "kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "ms": ms, "launches": nl, "unique_cs": r.total_rows,
-            "kernels": {q[0]: round(q[2], 3) for q in prof}}
+            "kernels": per}
 
 
 def cpu_baseline(inst, budget_s: float):
