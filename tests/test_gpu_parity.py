@@ -102,3 +102,42 @@ def test_cli_prints_reference_line(tmp_path):
     ref = oracle.solve(oracle.Problem.from_instance(inst))
     expect = synth.rpn_to_infix(ref["rpn"], inst.names)
     assert out.stdout == f"{path}, {expect}\n"
+
+
+# ----------------------------------------------------------------- edge cases
+def test_maximum_trace_count(engine):
+    # 128 traces (the build's limit; the P1 tile holds 129-word rows)
+    inst = cases.random_instance(7001, 3, 64, 64, [1 + (i * 7) % 12 for i in range(128)], 5)
+    _check(engine, inst)
+
+
+def test_maximum_proposition_count(engine):
+    # 64 propositions: 64 level-1 rows, a size-5 solution
+    inst = cases.random_instance(7137, 64, 10, 10, 8, 5)
+    _check(engine, inst)
+
+
+def test_duplicate_propositions(engine):
+    inst = cases.random_instance(7003, 3, 3, 3, 8, 6)
+    for _, words in inst.pos + inst.neg:
+        words[2] = words[0]          # p2 is p0 on every trace
+    _check(engine, inst)
+
+
+def test_single_trace_and_one_sided_samples(engine):
+    one = cases.random_instance(7004, 2, 1, 0, 5, 5)     # one positive trace only
+    _check(engine, one)
+    neg = cases.random_instance(7005, 2, 0, 3, 5, 5)     # negatives only
+    _check(engine, neg)
+
+
+def test_length_one_traces(engine):
+    inst = cases.random_instance(7006, 3, 4, 4, 1, 6)
+    _check(engine, inst)
+
+
+def test_exact_key_boundary(engine):
+    # trace lengths summing to exactly 126 bits (the last exact-key size) and
+    # to 127 (the first relaxed one)
+    _check(engine, cases.random_instance(7200, 2, 3, 3, [21] * 6, 7))
+    _check(engine, cases.random_instance(7300, 2, 3, 3, [21] * 5 + [22], 7))
