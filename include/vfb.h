@@ -100,6 +100,17 @@ vfb_status vfb_solve(void *ctx, const vfb_instance *inst, vfb_result *out);
 /* Solves n independent instances together; out[i] equals vfb_solve(inst[i]). */
 vfb_status vfb_batch_solve(void *ctx, const vfb_instance *inst, int n, vfb_result *out);
 
+/* vfb_solve, then, when nothing is found up to inst->max_size, the BS stage
+ * of LTL_BS (BS LTL_BS.cu:870-1067) up to size bs_max_size: ~ & |
+ * combinations of the cached formulas over their step-0 vectors (bit i = the
+ * formula holds at step 0 of trace i), searched in canonical order (sizes
+ * ascending; ~ over size c-1, then & and | over size splits i <= (c-1)/2,
+ * left index major) with the first occurrence of each vector kept; the first
+ * combination whose vector is exactly the positive traces' is returned.
+ * Sizes above max_size report vector entries in level_rows and combinations
+ * in level_cands.  At most 64 traces (VFB_LIMIT otherwise). */
+vfb_status vfb_solve_bs(void *ctx, const vfb_instance *inst, int bs_max_size, vfb_result *out);
+
 /* Cache-free search, replacing string LTL(...) of ltl_nocache.cu:319-446:
  * every formula of each size is evaluated in the numbering order of
  * numberToFormula (ltl_nocache.cu:169-224) with no cache and no

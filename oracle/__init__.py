@@ -138,6 +138,13 @@ def solve(prob: Problem) -> dict:
     return out
 
 
+def solve_bs(prob: Problem, bs_max: int) -> dict:
+    """solve(), then the BS stage up to size bs_max when nothing was found."""
+    r = _Result()
+    lib().orc_solve_bs(ctypes.byref(prob.p), bs_max, ctypes.byref(r))
+    return _result(r)
+
+
 def exhaustive(prob: Problem, max_formulas: int = 1 << 26) -> dict:
     r = _Result()
     lib().orc_exhaustive(ctypes.byref(prob.p), max_formulas, ctypes.byref(r))

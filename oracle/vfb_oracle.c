@@ -537,10 +537,9 @@ static int check_problem(const orc_problem *p) {
     return 1;
 }
 
-int orc_solve(const orc_problem *p, orc_result *res) {
-    memset(res, 0, sizeof(*res));
-    if (!check_problem(p)) return res->status = ORC_BAD_INPUT;
-    const double t0 = now_s();
+/* The cached search; leaves its state in *sp for a following BS stage (the
+ * caller frees it with search_free). */
+static int run_search(const orc_problem *p, orc_result *res, search_t *sp) {
     search_t s;
     memset(&s, 0, sizeof(s));
     s.p = p;
@@ -611,9 +610,171 @@ int orc_solve(const orc_problem *p, orc_result *res) {
     res->total_rows = s.rows.n;
     res->trace_len = s.trace_len;
 done:
-    kset_free(&s.set);
-    rows_free(&s.rows);
-    free(s.tmp);
+    *sp = s;
+    return res->status;
+}
+
+static void search_free(search_t *s) {
+    kset_free(&s->set);
+    rows_free(&s->rows);
+    free(s->tmp);
+}
+
+int orc_solve(const orc_problem *p, orc_result *res) {
+    memset(res, 0, sizeof(*res));
+    if (!check_problem(p)) return res->status = ORC_BAD_INPUT;
+    const double t0 = now_s();
+    search_t s;
+    run_search(p, res, &s);
+    search_free(&s);
+    res->seconds = now_s() - t0;
+    return res->status;
+}
+
+/* ------------------------------------------------------------------ BS stage
+ * After a search that found nothing up to max_size, LTL_BS combines the cached
+ * formulas with ~ & | over their step-0 vectors (BS LTL_BS.cu:870-1067):
+ * every cached CS projects to a word with bit i = the formula holds at step 0
+ * of trace i (transfer 808-822); a combination solves the sample when its word
+ * is exactly the positive traces' bits (BSInsertInCache 279-288).  Restated
+ * deterministically: the base entries of size c are the projections of the
+ * level-c rows not seen earlier in canonical order; sizes c > max_size hold
+ * ~ over size c-1, then & and | over size splits i <= (c-1)/2 (left index
+ * major), each new word kept, the first solving candidate returned. */
+typedef struct {
+    uint64_t *v;
+    int64_t *a, *b;
+    int8_t *op;      /* -1: base entry, a = cache row */
+    uint64_t n, cap;
+} bsrows_t;
+
+static int bs_push(bsrows_t *r, uint64_t v, int op, int64_t a, int64_t b) {
+    if (r->n == r->cap) {
+        uint64_t nc = r->cap ? 2 * r->cap : 1024;
+        uint64_t *nv = (uint64_t *)realloc(r->v, nc * sizeof(uint64_t));
+        if (!nv) return 0;
+        r->v = nv;
+        int64_t *na = (int64_t *)realloc(r->a, nc * sizeof(int64_t));
+        if (!na) return 0;
+        r->a = na;
+        int64_t *nb = (int64_t *)realloc(r->b, nc * sizeof(int64_t));
+        if (!nb) return 0;
+        r->b = nb;
+        int8_t *no = (int8_t *)realloc(r->op, nc);
+        if (!no) return 0;
+        r->op = no;
+        r->cap = nc;
+    }
+    r->v[r->n] = v;
+    r->op[r->n] = (int8_t)op;
+    r->a[r->n] = a;
+    r->b[r->n] = b;
+    r->n++;
+    return 1;
+}
+
+static void bs_rpn(const search_t *s, const bsrows_t *r, int64_t e, int16_t *out, int *n) {
+    if (r->op[e] < 0) {
+        rpn_of_row(s, r->a[e], out, n);
+        return;
+    }
+    bs_rpn(s, r, r->a[e], out, n);
+    if (r->op[e] != OP_NOT) bs_rpn(s, r, r->b[e], out, n);
+    out[(*n)++] = (int16_t)(-(1 + r->op[e]));
+}
+
+static int bs_stage(search_t *s, int bs_max, orc_result *res) {
+    const orc_problem *p = s->p;
+    const int T = s->T, K = p->max_size;
+    if (T > 64) return ORC_LIMIT;
+    const uint64_t full = T == 64 ? ~0ULL : ((1ULL << T) - 1);
+    const uint64_t target = p->num_pos == 64 ? ~0ULL : ((1ULL << p->num_pos) - 1);
+    uint64_t st[ORC_MAX_SIZE + 2], cn[ORC_MAX_SIZE + 2];
+    memset(st, 0, sizeof(st));
+    memset(cn, 0, sizeof(cn));
+    bsrows_t r;
+    memset(&r, 0, sizeof(r));
+    kset set;
+    int status = ORC_NOT_FOUND;
+    if (!kset_init(&set, 1 << 12)) return ORC_LIMIT;
+    for (int c = 1; c <= K; ++c) {
+        st[c] = r.n;
+        for (uint64_t i = 0; i < s->lvl_count[c]; ++i) {
+            const int64_t row = (int64_t)(s->lvl_start[c] + i);
+            const uint64_t *cs = row_cs(s, row);
+            uint64_t v = 0;
+            for (int t = 0; t < T; ++t) v |= (cs[t] & 1ULL) << t;
+            const int ins = kset_insert(&set, v & 0xffffffffULL, v >> 32);
+            if (ins < 0 || (ins && !bs_push(&r, v, -1, row, -1))) { status = ORC_LIMIT; goto out; }
+        }
+        cn[c] = r.n - st[c];
+    }
+    for (int c = K + 1; c <= bs_max; ++c) {
+        st[c] = r.n;
+        uint64_t cands = 0;
+        int64_t win = -1;
+        int wop = 0;
+        int64_t wa = -1, wb = -1;
+        for (int op = 0; op < 3 && win < 0; ++op) {
+            if (op == OP_NOT) {
+                for (uint64_t a = 0; a < cn[c - 1] && win < 0; ++a) {
+                    const int64_t ea = (int64_t)(st[c - 1] + a);
+                    const uint64_t v = ~r.v[ea] & full;
+                    ++cands;
+                    if (v == target) { win = (int64_t)cands - 1; wop = op; wa = ea; break; }
+                    const int ins = kset_insert(&set, v & 0xffffffffULL, v >> 32);
+                    if (ins < 0 || (ins && !bs_push(&r, v, op, ea, -1))) { status = ORC_LIMIT; goto out; }
+                }
+                continue;
+            }
+            for (int i = 1; 2 * i <= c - 1 && win < 0; ++i) {
+                const int j = c - 1 - i;
+                for (uint64_t a = 0; a < cn[i] && win < 0; ++a)
+                    for (uint64_t b = 0; b < cn[j]; ++b) {
+                        const int64_t ea = (int64_t)(st[i] + a), eb = (int64_t)(st[j] + b);
+                        const uint64_t v = op == OP_AND ? (r.v[ea] & r.v[eb]) : (r.v[ea] | r.v[eb]);
+                        ++cands;
+                        if (v == target) { win = (int64_t)cands - 1; wop = op; wa = ea; wb = eb; break; }
+                        const int ins = kset_insert(&set, v & 0xffffffffULL, v >> 32);
+                        if (ins < 0 || (ins && !bs_push(&r, v, op, ea, eb))) { status = ORC_LIMIT; goto out; }
+                    }
+            }
+        }
+        cn[c] = r.n - st[c];
+        res->level_rows[c] = cn[c];
+        res->level_cands[c] = cands;
+        res->size = c;
+        if (win >= 0) {
+            res->level_rows[c] = cn[c] + 1;
+            if (!bs_push(&r, target, wop, wa, wb)) { status = ORC_LIMIT; goto out; }
+            int n = 0;
+            bs_rpn(s, &r, (int64_t)r.n - 1, res->rpn, &n);
+            res->rpn_len = n;
+            res->solution_index = (uint64_t)win;
+            status = ORC_FOUND;
+            break;
+        }
+    }
+out:
+    res->total_rows = s->rows.n;
+    for (int c = K + 1; c <= res->size; ++c) res->total_rows += res->level_rows[c];
+    kset_free(&set);
+    free(r.v);
+    free(r.a);
+    free(r.b);
+    free(r.op);
+    return status;
+}
+
+int orc_solve_bs(const orc_problem *p, int bs_max, orc_result *res) {
+    memset(res, 0, sizeof(*res));
+    if (!check_problem(p) || bs_max > ORC_MAX_SIZE) return res->status = ORC_BAD_INPUT;
+    const double t0 = now_s();
+    search_t s;
+    run_search(p, res, &s);
+    if (res->status == ORC_NOT_FOUND && bs_max > p->max_size && p->mode == ORC_MODE_CANONICAL)
+        res->status = bs_stage(&s, bs_max, res);
+    search_free(&s);
     res->seconds = now_s() - t0;
     return res->status;
 }

@@ -71,6 +71,13 @@ typedef struct {
 /* Solve one instance.  Returns result->status. */
 int orc_solve(const orc_problem *p, orc_result *r);
 
+/* Solve, then, when nothing is found up to max_size, the BS stage of
+ * LTL_BS.cu:870-1067 up to size bs_max: ~ & | combinations of the cached
+ * formulas over their step-0 vectors (deterministic restatement, see the
+ * source).  Sizes above max_size report BS entries in level_rows and
+ * candidates in level_cands.  Needs at most 64 traces (ORC_LIMIT otherwise). */
+int orc_solve_bs(const orc_problem *p, int bs_max, orc_result *r);
+
 /* Exhaustive search in ltl_nocache numbering order (no cache, no dedup).
  * Returns the first formula (lowest number) that is a solution, or
  * ORC_NOT_FOUND / ORC_LIMIT when max_formulas candidates were evaluated. */

@@ -193,3 +193,21 @@ def test_refcompat_level3_candidates():
     assert can["level_cands"][2] == 4 * n2 + 3 * n1 * n1
     # LTL_BS: U covers even pairs of level1 x level1, both orientations
     assert ref["level_cands"][2] == 4 * n2 + 2 * n1 * n1 + 2 * ((n1 * n1 + 1) // 2)
+
+
+def test_bs_stage_returns_solutions():
+    # the BS stage's formulas are solutions, larger than the search's max size
+    from tests import cases as _cases
+    found = 0
+    for seed in range(8000, 8010):
+        inst = _cases.random_instance(seed, 3, 4, 4, [5, 6, 7, 8, 5, 6, 7, 8], 3)
+        p = oracle.Problem.from_instance(inst)
+        if oracle.solve(p)["status"] != oracle.NOT_FOUND:
+            continue
+        r = oracle.solve_bs(p, 8)
+        if r["status"] == oracle.FOUND:
+            found += 1
+            assert r["size"] > 3 and len(r["rpn"]) == r["size"]
+            assert oracle.eval_rpn(p, r["rpn"])[0] == 1
+            assert set(t for t in r["rpn"] if isinstance(t, str)) <= {"~", "&", "|", "X", "F", "G", "U"}
+    assert found >= 3

@@ -74,7 +74,7 @@ EXPORTS = ["vfb_create", "vfb_destroy", "vfb_solve", "vfb_batch_solve", "vfb_sta
            "vfb_read_json", "vfb_json_free", "vfb_format_infix", "vfb_profile_read",
            "vfb_profile_reset", "vfb_solve_noalloc", "vfb_synth_planted", "vfb_serve_open",
            "vfb_serve_limits", "vfb_serve_submit", "vfb_serve_step", "vfb_serve_close",
-           "vfb_solve_exhaustive"]
+           "vfb_solve_exhaustive", "vfb_solve_bs"]
 
 _lib = None
 
@@ -118,6 +118,8 @@ def load_library():
     lib.vfb_solve_noalloc.restype = ctypes.c_int
     lib.vfb_serve_open.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     lib.vfb_serve_open.restype = ctypes.c_int
+    lib.vfb_solve_bs.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Instance), ctypes.c_int, ctypes.POINTER(_Result)]
+    lib.vfb_solve_bs.restype = ctypes.c_int
     lib.vfb_solve_exhaustive.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Instance), ctypes.POINTER(_Result)]
     lib.vfb_solve_exhaustive.restype = ctypes.c_int
     lib.vfb_serve_limits.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_uint64, ctypes.c_uint64]
@@ -274,6 +276,14 @@ class Engine:
         inst, keep = prob._cstruct()
         res = _Result()
         self._lib.vfb_solve(self._ctx, ctypes.byref(inst), ctypes.byref(res))
+        del keep
+        return _result(res)
+
+    def solve_bs(self, prob: Problem, bs_max_size: int) -> Result:
+        """solve(), then the BS stage up to bs_max_size when nothing was found."""
+        inst, keep = prob._cstruct()
+        res = _Result()
+        self._lib.vfb_solve_bs(self._ctx, ctypes.byref(inst), bs_max_size, ctypes.byref(res))
         del keep
         return _result(res)
 

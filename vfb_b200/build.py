@@ -23,7 +23,8 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include")]
 
-UNITS = ["vfb_kernels.cu", "vfb_engine.cu", "vfb_io.cpp", "vfb_noalloc.cu", "vfb_synth.cpp", "vfb_exhaustive.cu"]
+UNITS = ["vfb_kernels.cu", "vfb_engine.cu", "vfb_io.cpp", "vfb_noalloc.cu", "vfb_synth.cpp", "vfb_exhaustive.cu",
+         "vfb_bs.cu"]
 HEADERS = ["vfb_device.cuh", "vfb_kernels.cuh", "vfb_ops.cuh"]
 
 

@@ -13,6 +13,8 @@
 //   --strict-exit  non-zero exit status on errors and when nothing is found
 //   --nocache      cache-free search in formula-number order (the reference's
 //                  ltl_nocache method) instead of the cached search
+//   --bs-max N     when nothing is found up to max size, the BS stage of LTL_BS
+//                  (~ & | over the cached formulas' step-0 vectors) up to size N
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -30,7 +32,7 @@ static void usage(const char* prog) {
 
 int main(int argc, char** argv) {
   std::vector<const char*> pos;
-  int rlx = 3, device = 0, stats = 0, quiet = 0, strict = 0, nocache = 0;
+  int rlx = 3, device = 0, stats = 0, quiet = 0, strict = 0, nocache = 0, bs_max = 0;
   double mem_gb = 0;
   for (int i = 1; i < argc; ++i) {
     const std::string a = argv[i];
@@ -41,6 +43,7 @@ int main(int argc, char** argv) {
     else if (a == "--quiet") quiet = 1;
     else if (a == "--strict-exit") strict = 1;
     else if (a == "--nocache") nocache = 1;
+    else if (a == "--bs-max" && i + 1 < argc) bs_max = std::atoi(argv[++i]);
     else pos.push_back(argv[i]);
   }
   if (pos.size() != 2) {
@@ -99,7 +102,9 @@ int main(int argc, char** argv) {
   inst.max_size = maxLen;
   inst.rlx_type = rlx;
   vfb_result res;
-  s = nocache ? vfb_solve_exhaustive(ctx, &inst, &res) : vfb_solve(ctx, &inst, &res);
+  if (nocache) s = vfb_solve_exhaustive(ctx, &inst, &res);
+  else if (bs_max > maxLen) s = vfb_solve_bs(ctx, &inst, bs_max, &res);
+  else s = vfb_solve(ctx, &inst, &res);
   int rc = 0;
   if (res.status == VFB_OK) {
     const int n = vfb_format_infix(&res, jp->names, nullptr, 0);

@@ -21,6 +21,7 @@
 #include <deque>
 #include <map>
 #include <new>
+#include <functional>
 #include <vector>
 
 #include "vfb_kernels.cuh"
@@ -1093,6 +1094,23 @@ struct Engine {
         }
       }
     }
+    if (bs_max > 0 && rc == VFB_OK) {
+      for (int i = 0; i < n; ++i) {
+        if (!H[i].d.rows || recs[i].status != ST_NOT_FOUND || bs_max <= recs[i].max_size) continue;
+        const vfb_status s = bs_stage(i, recs[i], out[i]);
+        if (s != VFB_OK) out[i].status = s;
+      }
+      float ms2 = 0;
+      cudaEventRecord(ev_t1, stream);
+      cudaStreamSynchronize(stream);
+      cudaEventElapsedTime(&ms2, ev_t0, ev_t1);
+      const double secs2 = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      for (int i = 0; i < n; ++i) {
+        out[i].device_seconds = ms2 * 1e-3;
+        out[i].seconds = secs2;
+        out[i].kernel_launches = c_launch;
+      }
+    }
     for (int i = 0; i < n; ++i) {
       if (!H[i].d.rows) continue;
       if (recs[i].status == ST_FOUND || recs[i].status == ST_NOT_FOUND) {
@@ -1385,6 +1403,267 @@ struct Engine {
     return VFB_OK;
   }
 
+  // ================================================================ BS stage
+  // After instance i (record d) found nothing up to its max size: ~ & |
+  // combinations of its cached formulas over their step-0 vectors, sizes up to
+  // bs_max (kernels in vfb_bs.cu).  Fills r's sizes above max_size; the
+  // instance's buffers must still be held.
+  int bs_max = 0;   // set by vfb_solve_bs for the call
+
+  vfb_status bs_stage(int i, const InstDev& d, vfb_result& r) {
+    const int K = d.max_size, T = d.T;
+    if (T > 64 || bs_max > kMaxSize) return VFB_LIMIT;
+    const uint64_t nrows = d.lstart[K] + d.lcount[K];
+    BsDev D;
+    std::memset(&D, 0, sizeof(D));
+    D.rows = d.rows;
+    D.T = T;
+    D.TP = d.TP;
+    D.full = T == 64 ? ~0ULL : ((1ULL << T) - 1);
+    D.target = d.npos == 64 ? ~0ULL : ((1ULL << d.npos) - 1);
+    std::vector<void*> held;
+    auto take = [&](size_t bytes) -> void* {
+      size_t g = 0;
+      void* p = dalloc(bytes, &g);
+      if (p) held.push_back(p);
+      return p;
+    };
+    auto release = [&]() { for (void* p : held) dfree(p); held.clear(); };
+    vfb_status rc = VFB_OK;
+    // entries of the base and of every size: at most one per cache row or candidate
+    uint64_t ent_cap = nrows + 1024, slots = pow2_at_least(4 * ent_cap), words_cap = (nrows + 31) / 32 + 1;
+    uint64_t chunk_cap = (words_cap + kBsChunkWords - 1) / kBsChunkWords + 1;
+    D.tab = (Slot*)take(slots * sizeof(Slot));
+    D.vals = (uint64_t*)take(ent_cap * 8);
+    D.org = (uint64_t*)take(ent_cap * 8);
+    D.bitmap = (uint32_t*)take(words_cap * 4);
+    D.counts = (unsigned long long*)take(chunk_cap * 8);
+    D.offs = (unsigned long long*)take(chunk_cap * 8);
+    D.best = (unsigned long long*)take(64);
+    D.fail = D.best + 1;
+    unsigned long long* bnd = (unsigned long long*)take(2 * (kMaxSize + 2) * 8);
+    if (!D.tab || !D.vals || !D.org || !D.bitmap || !D.counts || !D.offs || !D.best || !bnd) {
+      release();
+      return VFB_OOM;
+    }
+    D.mask = slots - 1;
+    cudaMemsetAsync(D.tab, 0xFF, slots * sizeof(Slot), stream);
+    cudaMemsetAsync(D.bitmap, 0, words_cap * 4, stream);
+    cudaMemsetAsync(D.best, 0xFF, 8, stream);
+    cudaMemsetAsync(D.fail, 0, 8, stream);
+    const int g256 = sms * 8;
+    std::vector<unsigned long long> hcount;
+    // compaction of the owner bits below nbits into entries from out0
+    auto compact = [&](int c, uint64_t nbits, uint64_t out0, uint64_t& n_out) -> vfb_status {
+      const uint64_t nwords = (nbits + 31) / 32;
+      const unsigned chunks = (unsigned)((nwords + kBsChunkWords - 1) / kBsChunkWords);
+      if (chunks == 0) { n_out = 0; return VFB_OK; }
+      k_bs_count<<<chunks, 256, 0, stream>>>(D, (unsigned long long)nwords);
+      hcount.assign(chunks, 0);
+      if (cudaMemcpyAsync(hcount.data(), D.counts, chunks * 8, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+          cudaStreamSynchronize(stream) != cudaSuccess)
+        return dev_fail(__LINE__);
+      unsigned long long run = 0;
+      for (unsigned j = 0; j < chunks; ++j) { const unsigned long long x = hcount[j]; hcount[j] = run; run += x; }
+      if (out0 + run > ent_cap) return VFB_OOM;
+      cudaMemcpyAsync(D.offs, hcount.data(), chunks * 8, cudaMemcpyHostToDevice, stream);
+      k_bs_emit<<<chunks, 256, 0, stream>>>(D, c, (unsigned long long)nwords, (unsigned long long)out0);
+      c_launch += 2;
+      n_out = run;
+      return VFB_OK;
+    };
+    // base entries: the rows' words, first occurrence in row order
+    k_bs_base<<<g256, 256, 0, stream>>>(D, (unsigned long long)nrows);
+    k_bs_mark<<<g256, 256, 0, stream>>>(D, 0, (unsigned long long)slots, (unsigned long long)nrows);
+    c_launch += 2;
+    uint64_t nent = 0;
+    rc = compact(0, nrows, 0, nent);
+    unsigned long long fails = 0;
+    if (rc == VFB_OK) {
+      std::vector<unsigned long long> at(K + 1), pos(K + 1);
+      for (int c = 1; c <= K; ++c) at[c - 1] = d.lstart[c];
+      at[K] = nrows;
+      cudaMemcpyAsync(bnd, at.data(), (K + 1) * 8, cudaMemcpyHostToDevice, stream);
+      k_bs_bounds<<<1, 64, 0, stream>>>(D, (unsigned long long)nent, bnd, K + 1, bnd + kMaxSize + 2);
+      ++c_launch;
+      cudaMemcpyAsync(pos.data(), bnd + kMaxSize + 2, (K + 1) * 8, cudaMemcpyDeviceToHost, stream);
+      cudaMemcpyAsync(&fails, D.fail, 8, cudaMemcpyDeviceToHost, stream);
+      if (cudaStreamSynchronize(stream) != cudaSuccess) rc = dev_fail(__LINE__);
+      for (int c = 1; c <= K; ++c) {
+        D.st[c] = pos[c - 1];
+        D.cn[c] = pos[c] - pos[c - 1];
+      }
+    }
+    if (rc == VFB_OK && fails) rc = VFB_LIMIT;
+    uint64_t total_bs = 0;
+    unsigned long long best = ~0ULL;
+    int c = K;
+    for (c = K + 1; rc == VFB_OK && c <= bs_max; ++c) {
+      // candidates of size c, in 128 bits against overflow
+      unsigned __int128 cands = D.cn[c - 1];
+      for (int a = 1; 2 * a <= c - 1; ++a) cands += 2 * (unsigned __int128)D.cn[a] * D.cn[c - 1 - a];
+      if (cands >= ((unsigned __int128)1 << 40)) { rc = VFB_LIMIT; break; }
+      const uint64_t nc = (uint64_t)cands;
+      // room: entries, table (at most half full), bitmap
+      if (nent + nc > ent_cap) {
+        const uint64_t want = nent + nc + 1024;
+        size_t g1 = 0, g2 = 0;
+        void* nv = dalloc(want * 8, &g1);
+        void* no = nv ? dalloc(want * 8, &g2) : nullptr;
+        if (!nv || !no) { dfree(nv); rc = VFB_OOM; break; }
+        cudaMemcpyAsync(nv, D.vals, nent * 8, cudaMemcpyDeviceToDevice, stream);
+        cudaMemcpyAsync(no, D.org, nent * 8, cudaMemcpyDeviceToDevice, stream);
+        for (void*& p : held) {
+          if (p == D.vals) { dfree(p); p = nv; }
+          else if (p == D.org) { dfree(p); p = no; }
+        }
+        D.vals = (uint64_t*)nv;
+        D.org = (uint64_t*)no;
+        ent_cap = want;
+      }
+      if (2 * (nent + nc) > slots) {
+        const uint64_t ns = pow2_at_least(4 * (nent + nc));
+        size_t g1 = 0;
+        void* pt = dalloc(ns * sizeof(Slot), &g1);
+        if (!pt) { rc = VFB_OOM; break; }
+        cudaMemsetAsync(pt, 0xFF, ns * sizeof(Slot), stream);
+        cudaMemsetAsync(D.fail, 0, 8, stream);
+        k_rehash<<<grid, 256, 0, stream>>>(D.tab, slots, (Slot*)pt, ns - 1, D.fail);
+        ++c_launch;
+        for (void*& p : held)
+          if (p == D.tab) { dfree(p); p = pt; }
+        D.tab = (Slot*)pt;
+        slots = ns;
+        D.mask = ns - 1;
+      }
+      const uint64_t nw = (nc + 31) / 32 + 1;
+      if (nw > words_cap) {
+        size_t g1 = 0, g2 = 0, g3 = 0;
+        void* pb = dalloc(nw * 4, &g1);
+        const uint64_t ncap = (nw + kBsChunkWords - 1) / kBsChunkWords + 1;
+        void* pc = pb ? dalloc(ncap * 8, &g2) : nullptr;
+        void* po = pc ? dalloc(ncap * 8, &g3) : nullptr;
+        if (!pb || !pc || !po) { dfree(pb); dfree(pc); rc = VFB_OOM; break; }
+        cudaMemsetAsync(pb, 0, nw * 4, stream);
+        for (void*& p : held) {
+          if (p == D.bitmap) { dfree(p); p = pb; }
+          else if (p == D.counts) { dfree(p); p = pc; }
+          else if (p == D.offs) { dfree(p); p = po; }
+        }
+        D.bitmap = (uint32_t*)pb;
+        D.counts = (unsigned long long*)pc;
+        D.offs = (unsigned long long*)po;
+        words_cap = nw;
+        chunk_cap = ncap;
+      }
+      cudaMemsetAsync(D.best, 0xFF, 8, stream);
+      k_bs_level<<<g256, 256, 0, stream>>>(D, c, (unsigned long long)nc);
+      ++c_launch;
+      cudaMemcpyAsync(&best, D.best, 8, cudaMemcpyDeviceToHost, stream);
+      cudaMemcpyAsync(&fails, D.fail, 8, cudaMemcpyDeviceToHost, stream);
+      if (cudaStreamSynchronize(stream) != cudaSuccess) { rc = dev_fail(__LINE__); break; }
+      if (fails) { rc = VFB_LIMIT; break; }
+      // new entries: the owners (below the solving candidate, if any)
+      const uint64_t lim = best != ~0ULL ? best : nc;
+      k_bs_mark<<<g256, 256, 0, stream>>>(D, c, (unsigned long long)slots, (unsigned long long)lim);
+      ++c_launch;
+      uint64_t nnew = 0;
+      rc = compact(c, lim, nent, nnew);
+      if (rc != VFB_OK) break;
+      D.st[c] = nent;
+      D.cn[c] = nnew;
+      nent += nnew;
+      r.level_rows[c] = nnew + (best != ~0ULL ? 1 : 0);
+      r.level_cands[c] = best != ~0ULL ? best + 1 : nc;
+      r.size = c;
+      total_bs += r.level_rows[c];
+      if (best != ~0ULL) break;
+    }
+    if (rc == VFB_OK && best != ~0ULL) {
+      // the formula: the solving candidate's tree over BS entries; its leaves
+      // are cache rows, rebuilt on the device
+      const int cs = r.size;
+      std::vector<uint64_t> orgs;
+      auto org_of = [&](uint64_t e) -> uint64_t {
+        uint64_t v = 0;
+        cudaMemcpy(&v, D.org + e, 8, cudaMemcpyDeviceToHost);
+        return v;
+      };
+      auto size_of = [&](uint64_t e) -> int {
+        for (int k = 1; k < cs; ++k)
+          if (e >= D.st[k] && e < D.st[k] + D.cn[k]) return k;
+        return -1;
+      };
+      struct Node { int op; int leaf; uint64_t a, b; };
+      std::vector<unsigned long long> leaves;
+      std::vector<int16_t> tokens;   // >= 0: leaf index + 1000; < 0: operator
+      std::function<bool(int, uint64_t, bool)> walk = [&](int k, uint64_t key, bool is_cand) -> bool {
+        // key: candidate index at size k (is_cand) or an entry index
+        uint64_t g = key;
+        if (!is_cand) {
+          k = size_of(key);
+          if (k < 0) return false;
+          g = org_of(key);
+          if (k <= K) {
+            leaves.push_back(g);   // g: cache row
+            tokens.push_back((int16_t)(1000 + leaves.size() - 1));
+            return true;
+          }
+        }
+        const BsCand cd = bs_decode(D.st, D.cn, k, g);
+        if (cd.op < 0) return false;
+        if (!walk(0, cd.a, false)) return false;
+        if (cd.op != OP_NOT && !walk(0, cd.b, false)) return false;
+        tokens.push_back((int16_t)(-(1 + cd.op)));
+        return true;
+      };
+      if (!walk(cs, best, true) || leaves.size() > (size_t)kMaxSize) {
+        rc = dev_fail(__LINE__);
+      } else {
+        const int nl = (int)leaves.size();
+        unsigned long long* dl = (unsigned long long*)take(nl * 8);
+        int16_t* drpn = (int16_t*)take((size_t)nl * kMaxSize * 2);
+        int* dlen = (int*)take(nl * 4);
+        if (!dl || !drpn || !dlen) {
+          rc = VFB_OOM;
+        } else {
+          cudaMemcpyAsync(dl, leaves.data(), nl * 8, cudaMemcpyHostToDevice, stream);
+          k_bs_leaves<<<1, 32, 0, stream>>>(dInst + i, dl, nl, drpn, dlen);
+          ++c_launch;
+          std::vector<int16_t> lr((size_t)nl * kMaxSize);
+          std::vector<int> ll(nl);
+          cudaMemcpyAsync(lr.data(), drpn, lr.size() * 2, cudaMemcpyDeviceToHost, stream);
+          cudaMemcpyAsync(ll.data(), dlen, nl * 4, cudaMemcpyDeviceToHost, stream);
+          if (cudaStreamSynchronize(stream) != cudaSuccess) rc = dev_fail(__LINE__);
+          int n = 0;
+          for (int16_t tk : tokens) {
+            if (rc != VFB_OK) break;
+            if (tk >= 1000) {
+              const int li = tk - 1000;
+              if (ll[li] <= 0 || n + ll[li] > kMaxSize) { rc = dev_fail(__LINE__); break; }
+              for (int j = 0; j < ll[li]; ++j) r.rpn[n++] = lr[(size_t)li * kMaxSize + j];
+            } else {
+              if (n >= kMaxSize) { rc = dev_fail(__LINE__); break; }
+              r.rpn[n++] = tk;
+            }
+          }
+          if (rc == VFB_OK && n == cs) {
+            r.rpn_len = n;
+            r.solution_index = best;
+            r.status = VFB_OK;
+          } else if (rc == VFB_OK) {
+            rc = dev_fail(__LINE__);
+          }
+        }
+      }
+    } else if (rc == VFB_OK) {
+      r.status = VFB_NOT_FOUND;
+    }
+    r.total_rows += total_bs;
+    release();
+    return rc;
+  }
+
   // ============================================================ cache-free search
   // Formula numbers of each size in order (ltl_nocache.cu:319-446), one launch
   // per range of kExhRange numbers; the first range with a solution gives the
@@ -1571,6 +1850,16 @@ void vfb_destroy(void* ctx) { delete static_cast<Engine*>(ctx); }
 vfb_status vfb_solve(void* ctx, const vfb_instance* inst, vfb_result* out) {
   if (!ctx || !inst || !out) return VFB_BAD_INPUT;
   const vfb_status rc = static_cast<Engine*>(ctx)->batch(inst, 1, out);
+  return rc != VFB_OK ? rc : out->status;
+}
+
+vfb_status vfb_solve_bs(void* ctx, const vfb_instance* inst, int bs_max_size, vfb_result* out) {
+  if (!ctx || !inst || !out) return VFB_BAD_INPUT;
+  if (bs_max_size < 1 || bs_max_size > VFB_MAX_SIZE) return VFB_BAD_INPUT;
+  Engine* e = static_cast<Engine*>(ctx);
+  e->bs_max = bs_max_size;
+  const vfb_status rc = e->batch(inst, 1, out);
+  e->bs_max = 0;
   return rc != VFB_OK ? rc : out->status;
 }
 

@@ -90,6 +90,55 @@ struct ExhDev {
 __global__ void k_exhaustive(const ExhDev* P, int k, unsigned long long lo, unsigned long long hi,
                              unsigned long long* best);
 
+// BS stage (vfb_bs.cu): words of the cache rows and of their ~ & |
+// combinations, in a slot table of their own.
+constexpr int kBsChunkWords = 1024;   // bitmap words per compaction chunk of the BS stage
+struct BsDev {
+  const uint64_t* rows;            // the instance's level cache (pitch TP)
+  int T, TP;
+  uint64_t full, target;           // T low bits; the positive traces' bits
+  Slot* tab;
+  unsigned long long mask;         // table capacity - 1
+  uint64_t* vals;                  // entries: words, in canonical order
+  uint64_t* org;                   // entries: cache row (base) or candidate index
+  uint32_t* bitmap;                // owner bits of the size being built
+  unsigned long long* counts;      // owners per chunk
+  unsigned long long* offs;        // chunk offsets (exclusive prefix of counts)
+  unsigned long long* best;        // first solving candidate of the size
+  unsigned long long* fail;        // probe failures
+  uint64_t st[kMaxSize + 2], cn[kMaxSize + 2];   // first entry and entries of each size
+};
+struct BsCand {
+  int op;
+  uint64_t a, b;   // entry indices of the operands
+};
+
+// Candidate g of BS size c -> operator and operand entries.
+__host__ __device__ inline BsCand bs_decode(const uint64_t* st, const uint64_t* cn, int c, uint64_t g) {
+  BsCand r{-1, 0, 0};
+  const uint64_t un = cn[c - 1];
+  if (g < un) return BsCand{OP_NOT, st[c - 1] + g, 0};
+  g -= un;
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int i = 1; 2 * i <= c - 1; ++i) {
+      const int j = c - 1 - i;
+      const uint64_t n = cn[i] * cn[j];
+      if (g < n) return BsCand{pass ? OP_OR : OP_AND, st[i] + g / cn[j], st[j] + g % cn[j]};
+      g -= n;
+    }
+  }
+  return r;
+}
+
+__global__ void k_bs_base(BsDev D, unsigned long long nrows);
+__global__ void k_bs_level(BsDev D, int c, unsigned long long cands);
+__global__ void k_bs_mark(BsDev D, int c, unsigned long long cap, unsigned long long limit);
+__global__ void k_bs_count(BsDev D, unsigned long long nwords);
+__global__ void k_bs_emit(BsDev D, int c, unsigned long long nwords, unsigned long long out0);
+__global__ void k_bs_bounds(BsDev D, unsigned long long nent, const unsigned long long* rows_at, int n,
+                            unsigned long long* out);
+__global__ void k_bs_leaves(const InstDev* I, const unsigned long long* rows, int n, int16_t* rpn, int* len);
+
 // Set-up and maintenance kernels.
 __global__ void k_init(BatchDev* B);
 __global__ void k_rehash(const Slot* old_tab, unsigned long long old_cap, Slot* new_tab,

@@ -453,20 +453,23 @@ __device__ __forceinline__ void warp_key(const InstDev& I, const Cand& c, int la
 }
 
 // RPN of the node (level lvl, candidate g) into I.rpn (postfix).
-__device__ inline void reconstruct(InstDev& I, int lvl, uint64_t g) {
+// RPN of candidate g of level lvl, rebuilt through the operands' canonical
+// indices (origin); returns its length (0 if it does not fit cap).
+__device__ inline int reconstruct_to(const InstDev& I, int lvl, uint64_t g, int16_t* rpn, int cap) {
   struct Fr { int lvl; uint64_t g; int state; };
   Fr st[2 * kMaxSize + 2];
   int sp = 0, out = 0;
   st[0] = {lvl, g, 0};
-  while (sp >= 0 && out < kMaxSize) {
+  while (sp >= 0) {
+    if (out >= cap) return 0;
     Fr& f = st[sp];
     if (f.lvl <= 1) {
-      I.rpn[out++] = (int16_t)f.g;
+      rpn[out++] = (int16_t)f.g;
       --sp;
       continue;
     }
     const Cand c = decode(I, f.lvl, f.g);
-    if (c.op < 0) { out = 0; break; }
+    if (c.op < 0) return 0;
     const bool bin = (c.op == OP_AND || c.op == OP_OR || c.op == OP_U);
     if (f.state == 0) {
       f.state = 1;
@@ -475,11 +478,15 @@ __device__ inline void reconstruct(InstDev& I, int lvl, uint64_t g) {
       f.state = 2;
       st[++sp] = {c.lb, I.origin[I.lstart[c.lb] + c.b], 0};
     } else {
-      I.rpn[out++] = (int16_t)(-(1 + c.op));
+      rpn[out++] = (int16_t)(-(1 + c.op));
       --sp;
     }
   }
-  I.rpn_len = out;
+  return out;
+}
+
+__device__ inline void reconstruct(InstDev& I, int lvl, uint64_t g) {
+  I.rpn_len = reconstruct_to(I, lvl, g, I.rpn, kMaxSize);
 }
 
 }  // namespace vfb
