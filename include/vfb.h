@@ -100,6 +100,19 @@ vfb_status vfb_solve(void *ctx, const vfb_instance *inst, vfb_result *out);
 /* Solves n independent instances together; out[i] equals vfb_solve(inst[i]). */
 vfb_status vfb_batch_solve(void *ctx, const vfb_instance *inst, int n, vfb_result *out);
 
+/* vfb_solve with the operator costs of LTL_BS (LTLI LTL_BS.cu:1069-1532,
+ * arguments c1..c8 and NegType of its main, 1612-1666): costs[0..7] = cost of
+ * a proposition, ~, &, |, X, F, G, U (each >= 1); the levels are then costs:
+ * a formula's cost is the sum of its symbols' costs, inst->max_size is the
+ * largest cost searched, and size / level_rows / level_cands are indexed by
+ * cost (levels below costs[0] are empty).  neg_type 1 lets ~ apply to any
+ * formula, 2 to propositions only.  The order within a cost is the reference's
+ * launch order: ~ & | X F G U, & and | over cost splits (i, k - c - i) with
+ * i <= k - c - i, U over every split, left index major.  Unit costs and
+ * neg_type 1 are exactly vfb_solve. */
+vfb_status vfb_solve_costs(void *ctx, const vfb_instance *inst, const int *costs, int neg_type,
+                           vfb_result *out);
+
 /* vfb_solve, then, when nothing is found up to inst->max_size, the BS stage
  * of LTL_BS (BS LTL_BS.cu:870-1067) up to size bs_max_size: ~ & |
  * combinations of the cached formulas over their step-0 vectors (bit i = the

@@ -42,7 +42,8 @@ class _Problem(ctypes.Structure):
                 ("max_rows", ctypes.c_uint64),
                 ("len", ctypes.POINTER(ctypes.c_uint8)),
                 ("atoms", ctypes.POINTER(ctypes.c_uint64)),
-                ("trace", ctypes.POINTER(ctypes.c_int64)), ("trace_cap", ctypes.c_int)]
+                ("trace", ctypes.POINTER(ctypes.c_int64)), ("trace_cap", ctypes.c_int),
+                ("cost", ctypes.c_int * 8), ("neg_type", ctypes.c_int)]
 
 
 class _Result(ctypes.Structure):
@@ -85,7 +86,7 @@ class Problem:
 
     def __init__(self, lengths, atoms, num_pos, max_size, rlx_type=3,
                  mode=CANONICAL, threads=1, ref_max_pitch=2147483647,
-                 max_rows=1 << 40):
+                 max_rows=1 << 40, costs=None, neg_type=1):
         t = len(lengths)
         a = len(atoms)
         self._len = (ctypes.c_uint8 * t)(*lengths)
@@ -96,7 +97,8 @@ class Problem:
                           ref_max_pitch, max_rows,
                           ctypes.cast(self._len, ctypes.POINTER(ctypes.c_uint8)),
                           ctypes.cast(self._atoms, ctypes.POINTER(ctypes.c_uint64)),
-                          ctypes.cast(self._trace, ctypes.POINTER(ctypes.c_int64)), 4096)
+                          ctypes.cast(self._trace, ctypes.POINTER(ctypes.c_int64)), 4096,
+                          (ctypes.c_int * 8)(*(costs or [1] * 8)), neg_type)
 
     @classmethod
     def from_instance(cls, inst, **kw):

@@ -320,18 +320,37 @@ static int process(search_t *s, int op, int64_t a, int64_t b) {
     return 0;
 }
 
-/* ---------------------------------------------------------- level: canonical */
+/* Operator cost (c2..c8 for ~ & | X F G U; c1 for a proposition). */
+static inline int op_cost(const orc_problem *p, int op) {
+    const int c = p->cost[1 + op];
+    return c > 0 ? c : 1;
+}
+static inline int atom_cost(const orc_problem *p) { return p->cost[0] > 0 ? p->cost[0] : 1; }
+
+/* ---------------------------------------------------------- level: canonical
+ * Level k holds the formulas of cost k (with unit costs: of size k).  Blocks
+ * ~ & | X F G U (LTL_BS.cu:1226-1488): a unary operator of cost c reads level
+ * k - c; & and | of cost c read splits (i, k - c - i), i from the
+ * propositions' cost while i <= k - c - i; U reads every split (i, k - c - i)
+ * with both sides at least the propositions' cost; left index major.  ~ reads
+ * only the propositions when neg_type is 2 (LTL_BS.cu:1237-1240). */
 static int level_canonical(search_t *s, int k) {
-    const uint64_t u0 = s->lvl_start[k - 1], un = s->lvl_count[k - 1];
+    const orc_problem *p = s->p;
+    const int c1 = atom_cost(p);
     for (int op = 0; op < 7; ++op) {
+        const int w = op_cost(p, op);
         if (op_is_unary(op)) {
+            const int L = k - w;
+            if (L < c1) continue;
+            if (op == OP_NOT && p->neg_type == 2 && L != c1) continue;
+            const uint64_t u0 = s->lvl_start[L], un = s->lvl_count[L];
             for (uint64_t a = 0; a < un; ++a)
                 if (process(s, op, (int64_t)(u0 + a), -1)) return 1;
             continue;
         }
-        const int last = (op == OP_U) ? k - 2 : (k - 1) / 2;
-        for (int i = 1; i <= last; ++i) {
-            const int j = k - 1 - i;
+        for (int i = c1; ; ++i) {
+            const int j = k - w - i;
+            if (j < c1 || (op != OP_U && i > j)) break;
             const uint64_t l0 = s->lvl_start[i], ln = s->lvl_count[i];
             const uint64_t r0 = s->lvl_start[j], rn = s->lvl_count[j];
             for (uint64_t a = 0; a < ln; ++a)
@@ -534,6 +553,14 @@ static int check_problem(const orc_problem *p) {
     if (p->rlx_type < 1 || p->rlx_type > 3) return 0;
     for (int i = 0; i < p->num_traces; ++i)
         if (p->len[i] < 1 || p->len[i] > 64) return 0;
+    int unit = p->neg_type == 0 || p->neg_type == 1;
+    if (p->neg_type < 0 || p->neg_type > 2) return 0;
+    for (int i = 0; i < 8; ++i) {
+        if (p->cost[i] < 0 || p->cost[i] > ORC_MAX_SIZE) return 0;
+        if (p->cost[i] > 1) unit = 0;
+    }
+    if (!unit && (p->mode != ORC_MODE_CANONICAL || p->threads > 1)) return 0;
+    if (atom_cost(p) > p->max_size) return 0;
     return 1;
 }
 
@@ -554,8 +581,9 @@ static int run_search(const orc_problem *p, orc_result *res, search_t *sp) {
     /* level 1: every proposition is a row (duplicates among them included),
      * its key enters the set, and each is tested as a size-1 solution in
      * proposition order (LTL_BS.cu:1127-1163, 1217). */
-    s.level = 1;
-    s.lvl_start[1] = 0;
+    const int c1 = atom_cost(p);
+    s.level = c1;
+    s.lvl_start[c1] = 0;
     trace_launch(&s, 1, 7, (uint64_t)p->num_vars);
     s.all_ltls = 0;
     for (int v = 0; v < p->num_vars; ++v) {
@@ -568,7 +596,7 @@ static int run_search(const orc_problem *p, orc_result *res, search_t *sp) {
         uint64_t h, l;
         make_key_s(p, s.S, cs, &h, &l);
         kset_insert(&s.set, h, l);
-        s.lvl_count[1]++;
+        s.lvl_count[c1]++;
         s.cands++;
         if (is_solution(p, cs)) {
             s.found = 1;
@@ -577,10 +605,11 @@ static int run_search(const orc_problem *p, orc_result *res, search_t *sp) {
             break;
         }
     }
-    res->level_rows[1] = s.lvl_count[1];
-    res->level_cands[1] = s.cands;
-    res->size = 1;
-    for (int k = 2; !s.found && k <= p->max_size; ++k) {
+    for (int k = 1; k <= c1; ++k) s.lvl_start[k] = 0;
+    res->level_rows[c1] = s.lvl_count[c1];
+    res->level_cands[c1] = s.cands;
+    res->size = c1;
+    for (int k = c1 + 1; !s.found && k <= p->max_size; ++k) {
         s.level = k;
         s.cands = 0;
         s.lvl_start[k] = s.rows.n;
@@ -769,6 +798,8 @@ out:
 int orc_solve_bs(const orc_problem *p, int bs_max, orc_result *res) {
     memset(res, 0, sizeof(*res));
     if (!check_problem(p) || bs_max > ORC_MAX_SIZE) return res->status = ORC_BAD_INPUT;
+    for (int i = 0; i < 8; ++i)
+        if (p->cost[i] > 1) return res->status = ORC_BAD_INPUT;   /* the BS stage uses unit costs */
     const double t0 = now_s();
     search_t s;
     run_search(p, res, &s);

@@ -53,6 +53,9 @@ typedef struct {
                                   (0..6, 7 = atoms), AllLTLs, StoredLTLs, ToBeChecked as
                                   printed before each launch (LTL_BS.cu:1193, 1230, ...) */
     int trace_cap;             /* launches the trace buffer can hold */
+    int cost[8];               /* operator costs c1..c8 of LTL_BS (p ~ & | X F G U); 0 = 1.
+                                  Levels are then costs: max_size is the maximum cost */
+    int neg_type;              /* 1: ~ of any formula; 2: ~ of propositions only; 0 = 1 */
 } orc_problem;
 
 typedef struct {

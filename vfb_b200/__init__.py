@@ -74,7 +74,7 @@ EXPORTS = ["vfb_create", "vfb_destroy", "vfb_solve", "vfb_batch_solve", "vfb_sta
            "vfb_read_json", "vfb_json_free", "vfb_format_infix", "vfb_profile_read",
            "vfb_profile_reset", "vfb_solve_noalloc", "vfb_synth_planted", "vfb_serve_open",
            "vfb_serve_limits", "vfb_serve_submit", "vfb_serve_step", "vfb_serve_close",
-           "vfb_solve_exhaustive", "vfb_solve_bs"]
+           "vfb_solve_exhaustive", "vfb_solve_bs", "vfb_solve_costs"]
 
 _lib = None
 
@@ -118,6 +118,9 @@ def load_library():
     lib.vfb_solve_noalloc.restype = ctypes.c_int
     lib.vfb_serve_open.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     lib.vfb_serve_open.restype = ctypes.c_int
+    lib.vfb_solve_costs.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Instance), ctypes.POINTER(ctypes.c_int),
+                                     ctypes.c_int, ctypes.POINTER(_Result)]
+    lib.vfb_solve_costs.restype = ctypes.c_int
     lib.vfb_solve_bs.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Instance), ctypes.c_int, ctypes.POINTER(_Result)]
     lib.vfb_solve_bs.restype = ctypes.c_int
     lib.vfb_solve_exhaustive.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Instance), ctypes.POINTER(_Result)]
@@ -276,6 +279,16 @@ class Engine:
         inst, keep = prob._cstruct()
         res = _Result()
         self._lib.vfb_solve(self._ctx, ctypes.byref(inst), ctypes.byref(res))
+        del keep
+        return _result(res)
+
+    def solve_costs(self, prob: Problem, costs, neg_type: int = 1) -> Result:
+        """solve() with LTL_BS's operator costs [p, ~, &, |, X, F, G, U] and NegType;
+        sizes in the result are then costs."""
+        inst, keep = prob._cstruct()
+        res = _Result()
+        arr = (ctypes.c_int * 8)(*costs)
+        self._lib.vfb_solve_costs(self._ctx, ctypes.byref(inst), arr, neg_type, ctypes.byref(res))
         del keep
         return _result(res)
 

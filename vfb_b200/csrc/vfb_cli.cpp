@@ -15,6 +15,10 @@
 //                  ltl_nocache method) instead of the cached search
 //   --bs-max N     when nothing is found up to max size, the BS stage of LTL_BS
 //                  (~ & | over the cached formulas' step-0 vectors) up to size N
+//   --costs c1,c2,c3,c4,c5,c6,c7,c8
+//                  LTL_BS's operator costs (p ~ & | X F G U); the max size is then
+//                  the largest cost searched
+//   --neg-type N   1: ~ of any formula (default); 2: ~ of propositions only
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -32,7 +36,9 @@ static void usage(const char* prog) {
 
 int main(int argc, char** argv) {
   std::vector<const char*> pos;
-  int rlx = 3, device = 0, stats = 0, quiet = 0, strict = 0, nocache = 0, bs_max = 0;
+  int rlx = 3, device = 0, stats = 0, quiet = 0, strict = 0, nocache = 0, bs_max = 0, neg_type = 1;
+  int costs[8] = {1, 1, 1, 1, 1, 1, 1, 1};
+  bool weighted = false;
   double mem_gb = 0;
   for (int i = 1; i < argc; ++i) {
     const std::string a = argv[i];
@@ -44,6 +50,18 @@ int main(int argc, char** argv) {
     else if (a == "--strict-exit") strict = 1;
     else if (a == "--nocache") nocache = 1;
     else if (a == "--bs-max" && i + 1 < argc) bs_max = std::atoi(argv[++i]);
+    else if (a == "--neg-type" && i + 1 < argc) { neg_type = std::atoi(argv[++i]); weighted = true; }
+    else if (a == "--costs" && i + 1 < argc) {
+      const std::string v = argv[++i];
+      size_t p0 = 0;
+      for (int c = 0; c < 8; ++c) {
+        const size_t p1 = v.find(',', p0);
+        costs[c] = std::atoi(v.substr(p0, p1 == std::string::npos ? std::string::npos : p1 - p0).c_str());
+        if (p1 == std::string::npos) break;
+        p0 = p1 + 1;
+      }
+      weighted = true;
+    }
     else pos.push_back(argv[i]);
   }
   if (pos.size() != 2) {
@@ -103,6 +121,7 @@ int main(int argc, char** argv) {
   inst.rlx_type = rlx;
   vfb_result res;
   if (nocache) s = vfb_solve_exhaustive(ctx, &inst, &res);
+  else if (weighted) s = vfb_solve_costs(ctx, &inst, costs, neg_type, &res);
   else if (bs_max > maxLen) s = vfb_solve_bs(ctx, &inst, bs_max, &res);
   else s = vfb_solve(ctx, &inst, &res);
   int rc = 0;

@@ -14,7 +14,9 @@ namespace vfb {
 constexpr int kMaxTraces = 128;
 constexpr int kMaxSize = 32;          // formula size limit (ltl_nocache.cu:11)
 constexpr int kMaxSplits = 16;        // floor((32-1)/2)
-constexpr int kGroups = 1 + kMaxSplits;
+// P1 operand groups of a level: up to 4 unary (one per operand level) and the
+// binary level pairs; with unit costs, 1 + floor((k-1)/2)
+constexpr int kGroups = 64;
 constexpr int kTS = 128;              // stream rows per P1 tile (= threads per CTA)
 constexpr int kTQ = 32;               // staged rows per P1 tile (maximum)
 constexpr int kP1TileTarget = 1024;   // shrink the staged height until a level has this many tiles
@@ -57,6 +59,9 @@ struct InstDev {
   uint8_t off[kMaxTraces];     // bit offset of the trace's key field (<=126)
   uint8_t width[kMaxTraces];   // key field width (0 when past bit 126)
   uint64_t posmask[2];         // bit i: trace i is positive
+  uint8_t cost[8];             // operator costs c1..c8 of LTL_BS (p ~ & | X F G U); 0 means 1.
+                               // Level k holds the formulas of cost k (unit costs: size k)
+  int neg_type;                // 2: ~ applies to propositions only (LTL_BS NegType)
   // ---- buffers (host-owned allocations; pointers may change between levels)
   uint64_t* rows;              // [row_cap][TP]
   uint64_t* origin;            // [row_cap] candidate index within the row's level
@@ -76,11 +81,15 @@ struct InstDev {
   uint64_t keys;               // keys in the table
   uint64_t cands;              // candidates of the level being built
   uint64_t base_not, base_x, base_f, base_g;
-  uint64_t base_and[kMaxSplits + 1], base_or[kMaxSplits + 1];
+  uint64_t base_and[kMaxSize + 1], base_or[kMaxSize + 1];   // indexed by the left operand's level
   uint64_t base_u[kMaxSize];
   // P1 tile groups: group 0 = unary over level k-1, group s = split s
   uint64_t grp_prefix[kGroups + 1];
   uint32_t grp_qtiles[kGroups];
+  // group g: kind 0 = unary over level la (mask bits ~ X F G), kind 1 = binary
+  // over levels la <= lb (mask bits &, |, la U lb, lb U la)
+  uint8_t grp_kind[kGroups], grp_mask[kGroups], grp_la[kGroups], grp_lb[kGroups];
+  int ngroups;
   int tq;                      // staged rows per P1 tile at this level (1..kTQ)
   int pad1;
   unsigned long long promote_above;  // candidates per level above which the instance
@@ -198,6 +207,18 @@ __device__ __forceinline__ void key_final(const KeyAcc& k, uint64_t& h, uint64_t
 
 __device__ __forceinline__ uint64_t slot_hash(uint64_t h, uint64_t l) {
   return splitmix_fin(h ^ (l * 0x9E3779B97F4A7C15ULL) ^ 0x5ad0dedULL);
+}
+
+// Operator cost (op index into ~ & | X F G U) and the propositions' cost
+// (their level); 0 in the record means 1.
+__host__ __device__ __forceinline__ int op_cost(const InstDev& I, int op) {
+  return I.cost[1 + op] ? I.cost[1 + op] : 1;
+}
+__host__ __device__ __forceinline__ int atom_level(const InstDev& I) { return I.cost[0] ? I.cost[0] : 1; }
+// Operand level of ~ at level k, or -1 when ~ has no candidates there.
+__host__ __device__ __forceinline__ int not_level(const InstDev& I, int k) {
+  const int L = k - op_cost(I, OP_NOT), c1 = atom_level(I);
+  return (L < c1 || (I.neg_type == 2 && L != c1)) ? -1 : L;
 }
 
 __device__ __forceinline__ bool is_pos(const InstDev& I, int i) {

@@ -829,6 +829,10 @@ struct Engine {
       }
       off += width[i];
     }
+    // operator costs of the call (vfb_solve_costs), else unit costs
+    for (int c = 0; c < 8; ++c) d.cost[c] = (uint8_t)req_cost[c];
+    d.neg_type = req_neg;
+    if (atom_level(d) > d.max_size) return VFB_BAD_INPUT;
     d.status = ST_RUNNING;
     d.level = 1;
     return VFB_OK;
@@ -1080,7 +1084,7 @@ struct Engine {
         r.rpn_len = d.rpn_len;
         for (int j = 0; j < d.rpn_len && j < kMaxSize; ++j) r.rpn[j] = d.rpn[j];
         r.solution_index = d.sol_index;
-        if (d.rpn_len != d.res_size) r.status = VFB_DEVICE_ERROR;
+        if (d.rpn_len < 1 || rpn_cost(d, d.rpn, d.rpn_len) != d.res_size) r.status = VFB_DEVICE_ERROR;
       } else if (d.status == ST_NOT_FOUND) {
         r.status = VFB_NOT_FOUND;
       } else {
@@ -1409,10 +1413,21 @@ struct Engine {
   // bs_max (kernels in vfb_bs.cu).  Fills r's sizes above max_size; the
   // instance's buffers must still be held.
   int bs_max = 0;   // set by vfb_solve_bs for the call
+  int req_cost[8] = {1, 1, 1, 1, 1, 1, 1, 1};   // set by vfb_solve_costs for the call
+  int req_neg = 1;
+
+  // Cost of an RPN formula under an instance's operator costs.
+  static int rpn_cost(const InstDev& d, const int16_t* rpn, int n) {
+    int c = 0;
+    for (int j = 0; j < n; ++j) c += rpn[j] >= 0 ? atom_level(d) : op_cost(d, -rpn[j] - 1);
+    return c;
+  }
 
   vfb_status bs_stage(int i, const InstDev& d, vfb_result& r) {
     const int K = d.max_size, T = d.T;
     if (T > 64 || bs_max > kMaxSize) return VFB_LIMIT;
+    for (int c = 0; c < 8; ++c)
+      if (d.cost[c] > 1) return VFB_BAD_INPUT;   // the BS stage uses unit costs
     const uint64_t nrows = d.lstart[K] + d.lcount[K];
     BsDev D;
     std::memset(&D, 0, sizeof(D));
@@ -1850,6 +1865,20 @@ void vfb_destroy(void* ctx) { delete static_cast<Engine*>(ctx); }
 vfb_status vfb_solve(void* ctx, const vfb_instance* inst, vfb_result* out) {
   if (!ctx || !inst || !out) return VFB_BAD_INPUT;
   const vfb_status rc = static_cast<Engine*>(ctx)->batch(inst, 1, out);
+  return rc != VFB_OK ? rc : out->status;
+}
+
+vfb_status vfb_solve_costs(void* ctx, const vfb_instance* inst, const int* costs, int neg_type, vfb_result* out) {
+  if (!ctx || !inst || !out || !costs) return VFB_BAD_INPUT;
+  if (neg_type != 1 && neg_type != 2) return VFB_BAD_INPUT;
+  for (int c = 0; c < 8; ++c)
+    if (costs[c] < 1 || costs[c] > VFB_MAX_SIZE) return VFB_BAD_INPUT;
+  Engine* e = static_cast<Engine*>(ctx);
+  for (int c = 0; c < 8; ++c) e->req_cost[c] = costs[c];
+  e->req_neg = neg_type;
+  const vfb_status rc = e->batch(inst, 1, out);
+  for (int c = 0; c < 8; ++c) e->req_cost[c] = 1;
+  e->req_neg = 1;
   return rc != VFB_OK ? rc : out->status;
 }
 

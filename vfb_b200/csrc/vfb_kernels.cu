@@ -49,19 +49,80 @@ __device__ __forceinline__ void step_entry() {
 // tiling, buffer checks.  Records the plan (planned = k, plan_*) or asks the
 // host for memory (NEED_MEM, planned = 0).
 __device__ void plan_one(InstDev& I) {
-  const int k = I.level;
+  const int k = I.level, c1 = atom_level(I);
   const uint64_t* n = I.lcount;
   I.lstart[k] = I.lstart[k - 1] + n[k - 1];
+  // candidate blocks in canonical order: ~ & | X F G U; a unary operator of
+  // cost c reads level k - c, & | over splits (i, k - c - i) with i <= k - c - i,
+  // U over every split (LTL_BS.cu:1226-1488; unit costs: the size order)
   uint64_t g = 0;
+  const int Ln = not_level(I, k);
   I.base_not = g;
-  g += n[k - 1];
-  for (int i = 1; 2 * i <= k - 1; ++i) { I.base_and[i] = g; g += n[i] * n[k - 1 - i]; }
-  for (int i = 1; 2 * i <= k - 1; ++i) { I.base_or[i] = g; g += n[i] * n[k - 1 - i]; }
-  I.base_x = g; g += n[k - 1];
-  I.base_f = g; g += n[k - 1];
-  I.base_g = g; g += n[k - 1];
-  for (int i = 1; i <= k - 2; ++i) { I.base_u[i] = g; g += n[i] * n[k - 1 - i]; }
+  if (Ln >= 0) g += n[Ln];
+  for (int pass = 0; pass < 2; ++pass) {
+    const int w = op_cost(I, pass ? OP_OR : OP_AND);
+    for (int i = c1; 2 * i <= k - w; ++i) {
+      const int j = k - w - i;
+      (pass ? I.base_or : I.base_and)[i] = g;
+      g += n[i] * n[j];
+    }
+  }
+  uint64_t* const ub[3] = {&I.base_x, &I.base_f, &I.base_g};
+  for (int o = 0; o < 3; ++o) {
+    const int L = k - op_cost(I, OP_X + o);
+    *ub[o] = g;
+    if (L >= c1) g += n[L];
+  }
+  {
+    const int w = op_cost(I, OP_U);
+    for (int i = c1; k - w - i >= c1; ++i) {
+      I.base_u[i] = g;
+      g += n[i] * n[k - w - i];
+    }
+  }
   I.cands = g;
+  // operand groups: the unary operators by operand level (bits ~ X F G), the
+  // binary ones by level pair la <= lb (bits &, |, la U lb, lb U la); with
+  // unit costs one unary group and one group per split, as the reference's
+  // launches fuse them
+  int ng = 0;
+  auto unary = [&](int L, int bit) {
+    if (L < c1) return;
+    for (int q = 0; q < ng; ++q)
+      if (I.grp_kind[q] == 0 && I.grp_la[q] == L) { I.grp_mask[q] |= (uint8_t)(1 << bit); return; }
+    if (ng >= kGroups) return;
+    I.grp_kind[ng] = 0; I.grp_la[ng] = (uint8_t)L; I.grp_lb[ng] = 0; I.grp_mask[ng] = (uint8_t)(1 << bit);
+    ++ng;
+  };
+  auto binary = [&](int la, int lb, int bits) {
+    for (int q = 0; q < ng; ++q)
+      if (I.grp_kind[q] == 1 && I.grp_la[q] == la && I.grp_lb[q] == lb) { I.grp_mask[q] |= (uint8_t)bits; return; }
+    if (ng >= kGroups) return;
+    I.grp_kind[ng] = 1; I.grp_la[ng] = (uint8_t)la; I.grp_lb[ng] = (uint8_t)lb; I.grp_mask[ng] = (uint8_t)bits;
+    ++ng;
+  };
+  unary(Ln, 0);
+  unary(k - op_cost(I, OP_X), 1);
+  unary(k - op_cost(I, OP_F), 2);
+  unary(k - op_cost(I, OP_G), 3);
+  {
+    const int s3 = k - op_cost(I, OP_AND), s4 = k - op_cost(I, OP_OR), s8 = k - op_cost(I, OP_U);
+    const int sums[3] = {s3, s4, s8};
+    for (int q = 0; q < 3; ++q) {
+      const int sm = sums[q];
+      if (q == 1 && sm == s3) continue;
+      if (q == 2 && (sm == s3 || sm == s4)) continue;
+      for (int i = c1; 2 * i <= sm; ++i) {
+        const int j = sm - i;
+        int bits = 0;
+        if (sm == s3) bits |= 1;
+        if (sm == s4) bits |= 2;
+        if (sm == s8) bits |= (i == j) ? 4 : (4 | 8);
+        binary(i, j, bits);
+      }
+    }
+  }
+  I.ngroups = ng;
   // P1 tiling: kTS stream rows x tq staged rows per tile; small levels get
   // shorter tiles so that they still spread over every SM
   // (tq is a power of two: tile counts by shifts, not 64-bit divisions)
@@ -69,20 +130,22 @@ __device__ void plan_one(InstDev& I) {
   int lg = 0;
   while ((1 << (lg + 1)) <= kTQ) ++lg;
   for (;;) {
-    t = (n[k - 1] + kTS - 1) / kTS;
+    t = 0;
     I.grp_prefix[0] = 0;
-    I.grp_prefix[1] = t;
-    for (int i = 1; i < kGroups; ++i) {
-      if (2 * i <= k - 1) {
-        const int j = k - 1 - i;
+    for (int q = 0; q < ng; ++q) {
+      if (I.grp_kind[q] == 0) {
+        t += (n[I.grp_la[q]] + kTS - 1) / kTS;
+      } else {
+        const int i = I.grp_la[q], j = I.grp_lb[q];
         const bool qleft = (i == j) || (n[i] <= n[j]);
         const uint64_t nS = qleft ? n[j] : n[i], nQ = qleft ? n[i] : n[j];
         const uint64_t qt = (nQ + (1ULL << lg) - 1) >> lg, st = (nS + kTS - 1) / kTS;
-        I.grp_qtiles[i] = (uint32_t)qt;
+        I.grp_qtiles[q] = (uint32_t)qt;
         t += st * qt;
       }
-      I.grp_prefix[i + 1] = t;
+      I.grp_prefix[q + 1] = t;
     }
+    for (int q = ng; q < kGroups; ++q) I.grp_prefix[q + 1] = t;
     if (t >= (uint64_t)kP1TileTarget || lg == 0) break;
     --lg;
   }
@@ -178,20 +241,27 @@ __device__ void ph_p1(const BatchDev& B) {
         const int b = find_owner(B.p1_prefix, B.ninst, tile);
         const InstDev* Ip = B.inst + b;
         const uint64_t local = tile - B.p1_prefix[b] + __ldcg(&Ip->p1_done);
-        const uint64_t gpl = (lane >= 1 && lane < kGroups) ? __ldcg(&Ip->grp_prefix[lane]) : ~0ULL;
-        const int grp = __popc(__ballot_sync(0xffffffffu, gpl <= local));
-        const uint64_t gstart = __shfl_sync(0xffffffffu, gpl, grp);
+        // lane l holds group boundaries 2l+1 and 2l+2; the group is the number
+        // of boundaries at or below the tile
+        const int e1 = 2 * lane + 1, e2 = 2 * lane + 2;
+        const uint64_t gp1 = e1 < kGroups ? __ldcg(&Ip->grp_prefix[e1]) : ~0ULL;
+        const uint64_t gp2 = e2 < kGroups ? __ldcg(&Ip->grp_prefix[e2]) : ~0ULL;
+        const int grp = __popc(__ballot_sync(0xffffffffu, gp1 <= local)) +
+                        __popc(__ballot_sync(0xffffffffu, gp2 <= local));
+        const int src = grp >= 1 ? (grp - 1) >> 1 : 0;
+        const uint64_t s1 = __shfl_sync(0xffffffffu, gp1, src), s2 = __shfl_sync(0xffffffffu, gp2, src);
+        const uint64_t gstart = grp == 0 ? 0 : ((grp & 1) ? s1 : s2);
         if (lane == 0) {
           const int k = __ldcg(&Ip->level), T = __ldcg(&Ip->T), TP = __ldcg(&Ip->TP);
           const int stride = __ldcg(&Ip->stride1), mode = __ldcg(&Ip->key_mode), tq = __ldcg(&Ip->tq);
           const uint64_t pos0 = __ldcg(&Ip->posmask[0]), pos1 = __ldcg(&Ip->posmask[1]);
           const unsigned long long cap = __ldcg(&Ip->table_mask) + 1, keys = __ldcg(&Ip->keys);
           const unsigned long long fails = __ldcg(&Ip->probe_fail), fresh = __ldcg(&Ip->n_new);
-          const int i = grp, j = k - 1 - grp;
-          const uint64_t nk1 = __ldcg(&Ip->lcount[k - 1]);
-          const uint64_t ni = grp ? __ldcg(&Ip->lcount[i]) : 0, nj = grp ? __ldcg(&Ip->lcount[j]) : 0;
-          const uint64_t qt = grp ? __ldcg(&Ip->grp_qtiles[grp]) : 1;
-          const uint64_t within = local - (grp ? gstart : 0);
+          const int kind = __ldcg(&Ip->grp_kind[grp]), gmask = __ldcg(&Ip->grp_mask[grp]);
+          const int i = __ldcg(&Ip->grp_la[grp]), j = __ldcg(&Ip->grp_lb[grp]);
+          const uint64_t ni = __ldcg(&Ip->lcount[i]), nj = kind ? __ldcg(&Ip->lcount[j]) : 0;
+          const uint64_t qt = kind ? __ldcg(&Ip->grp_qtiles[grp]) : 1;
+          const uint64_t within = local - gstart;
           P.inst = b;
           P.grp = grp;
           P.k = k;
@@ -205,9 +275,11 @@ __device__ void ph_p1(const BatchDev& B) {
           P.pos[1] = pos1;
           // give up early once the table is known to be too small for this level
           P.skip = (fails != 0) || (4 * (keys + fresh) > 3 * cap);
-          if (grp == 0) {
-            P.si = k - 1;
-            P.nS = nk1;
+          P.kind = kind;
+          P.mask = gmask;
+          if (kind == 0) {
+            P.si = i;
+            P.nS = ni;
             P.s0 = within * kTS;
           } else {
             const int qleft = (i == j) || (ni <= nj);
@@ -243,7 +315,7 @@ __device__ void ph_p1(const BatchDev& B) {
     if (!P.skip) {
       const int ns = (int)((P.nS - P.s0) < (uint64_t)kTS ? (P.nS - P.s0) : (uint64_t)kTS);
       stage_rows(sS, sp, row_ptr(I, P.si, P.s0), ns, P.TP);
-      if (P.grp > 0) {
+      if (P.kind == 1) {
         const int nq = (int)((P.nQ - P.q0) < (uint64_t)P.tq ? (P.nQ - P.q0) : (uint64_t)P.tq);
         stage_rows(sQ, P.TP, row_ptr(I, P.qi, P.q0), nq, P.TP);
       }
@@ -251,20 +323,20 @@ __device__ void ph_p1(const BatchDev& B) {
     }
     __syncthreads();
     if (!P.skip) {
-      const bool four = P.grp > 0 && P.i != P.j;
+      const bool four = P.kind == 1 && (P.mask & 8);
       switch (P.mode) {
         case KEY_HASH:
-          if (P.grp == 0) p1_unary<KEY_HASH>(I, P, sS, sp, cnt);
+          if (P.kind == 0) p1_unary<KEY_HASH>(I, P, sS, sp, cnt);
           else if (four) p1_binary<KEY_HASH, true>(I, P, sS, sp, sQ, cnt);
           else p1_binary<KEY_HASH, false>(I, P, sS, sp, sQ, cnt);
           break;
         case KEY_SAMPLED:
-          if (P.grp == 0) p1_unary<KEY_SAMPLED>(I, P, sS, sp, cnt);
+          if (P.kind == 0) p1_unary<KEY_SAMPLED>(I, P, sS, sp, cnt);
           else if (four) p1_binary<KEY_SAMPLED, true>(I, P, sS, sp, sQ, cnt);
           else p1_binary<KEY_SAMPLED, false>(I, P, sS, sp, sQ, cnt);
           break;
         default:
-          if (P.grp == 0) p1_unary<KEY_CONCAT>(I, P, sS, sp, cnt);
+          if (P.kind == 0) p1_unary<KEY_CONCAT>(I, P, sS, sp, cnt);
           else if (four) p1_binary<KEY_CONCAT, true>(I, P, sS, sp, sQ, cnt);
           else p1_binary<KEY_CONCAT, false>(I, P, sS, sp, sQ, cnt);
       }
@@ -1077,7 +1149,8 @@ __global__ void k_init(BatchDev* Bp) {
       row_key(I, row, h, l);
       int isnew = 0;
       uint64_t idx = slot_hash(h, l) & I.table_mask;
-      const int r = insert_min(I.table, I.table_mask, idx, ld_key(I.table + idx), h, l, pay_of(1, v), isnew);
+      const int r = insert_min(I.table, I.table_mask, idx, ld_key(I.table + idx), h, l,
+                               pay_of(atom_level(I), v), isnew);
       if (r < 0) atomicAdd(&I.probe_fail, 1ULL);
       if (isnew) atomicAdd(&s_new, 1ULL);
       I.origin[v] = v;
@@ -1087,26 +1160,31 @@ __global__ void k_init(BatchDev* Bp) {
     }
     __syncthreads();
     if (threadIdx.x == 0) {
+      // the propositions are the level of their cost c1 (1 with unit costs);
+      // the levels below it are empty
+      const int c1 = atom_level(I);
       I.keys = s_new;
-      I.lstart[0] = 0;
-      I.lcount[0] = 0;
-      I.lstart[1] = 0;
-      I.lcount[1] = I.A;
-      I.lcands[1] = I.A;
-      I.res_size = 1;
+      for (int k = 0; k <= c1; ++k) {
+        I.lstart[k] = 0;
+        I.lcount[k] = 0;
+        I.lcands[k] = 0;
+      }
+      I.lcount[c1] = I.A;
+      I.lcands[c1] = I.A;
+      I.res_size = c1;
       if (I.probe_fail) {
         I.status = ST_ERROR;
       } else if (s_first != ~0ULL) {
-        I.lcount[1] = s_first + 1;
-        I.lcands[1] = s_first + 1;
+        I.lcount[c1] = s_first + 1;
+        I.lcands[c1] = s_first + 1;
         I.sol_index = s_first;
         I.rpn[0] = (int16_t)s_first;
         I.rpn_len = 1;
         I.status = ST_FOUND;
-      } else if (I.max_size <= 1) {
+      } else if (I.max_size <= c1) {
         I.status = ST_NOT_FOUND;
       } else {
-        I.level = 2;
+        I.level = c1 + 1;
       }
       B.status_out[b] = make_int2(I.status, I.need);
     }

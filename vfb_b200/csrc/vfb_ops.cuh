@@ -144,19 +144,25 @@ __device__ __forceinline__ void divmod64(uint64_t g, uint64_t n, uint64_t& q, ui
 }
 
 // Canonical candidate index g of level k -> operator and operands (levels and
-// indices within them).  Block order ~ & | X F G U; & and | over left sizes
-// 1..floor((k-1)/2), U over 1..k-2; left index major (ltl_nocache.cu:169-224).
+// indices within them).  Block order ~ & | X F G U; a unary operator of cost
+// c reads level k - c; & and | over splits (i, k - c - i) with i <= k - c - i,
+// U over every split; left index major (ltl_nocache.cu:169-224 with unit
+// costs, LTL_BS.cu:1226-1488 with the operator costs).
 __device__ inline Cand decode(const InstDev& I, int k, uint64_t g) {
   const uint64_t* n = I.lcount;
+  const int c1 = atom_level(I);
   Cand c;
   c.lb = 0;
   c.b = 0;
-  const uint64_t un = n[k - 1];
-  if (g < un) { c.op = OP_NOT; c.la = k - 1; c.a = g; return c; }
-  g -= un;
+  const int Ln = not_level(I, k);
+  if (Ln >= 0) {
+    if (g < n[Ln]) { c.op = OP_NOT; c.la = Ln; c.a = g; return c; }
+    g -= n[Ln];
+  }
   for (int pass = 0; pass < 2; ++pass) {
-    for (int i = 1; 2 * i <= k - 1; ++i) {
-      const int j = k - 1 - i;
+    const int w = op_cost(I, pass ? OP_OR : OP_AND);
+    for (int i = c1; 2 * i <= k - w; ++i) {
+      const int j = k - w - i;
       const uint64_t cnt = n[i] * n[j];
       if (g < cnt) {
         c.op = pass ? OP_OR : OP_AND;
@@ -168,11 +174,14 @@ __device__ inline Cand decode(const InstDev& I, int k, uint64_t g) {
     }
   }
   for (int op = OP_X; op <= OP_G; ++op) {
-    if (g < un) { c.op = op; c.la = k - 1; c.a = g; return c; }
-    g -= un;
+    const int L = k - op_cost(I, op);
+    if (L < c1) continue;
+    if (g < n[L]) { c.op = op; c.la = L; c.a = g; return c; }
+    g -= n[L];
   }
-  for (int i = 1; i <= k - 2; ++i) {
-    const int j = k - 1 - i;
+  const int w = op_cost(I, OP_U);
+  for (int i = c1; k - w - i >= c1; ++i) {
+    const int j = k - w - i;
     const uint64_t cnt = n[i] * n[j];
     if (g < cnt) {
       c.op = OP_U; c.la = i; c.lb = j;
@@ -231,6 +240,7 @@ __device__ inline void row_key(const InstDev& I, const uint64_t* row, uint64_t& 
 struct TileSh {
   unsigned long long tile;
   int inst, grp, k, T, TP, half, stride, mode, skip;
+  int kind, mask;   // operand group: 0 unary / 1 binary; the operators it evaluates
   uint64_t s0, q0, nS, nQ, ni, nj;
   int si, qi;   // levels of the stream / staged operand
   int qleft;    // staged operand is the left operand of & | and of U(i->j)
@@ -268,7 +278,7 @@ struct P1Count {
 template <int N>
 __device__ __forceinline__ void insert_group(InstDev& I, unsigned live, int k, const uint64_t* h,
                                              const uint64_t* l, const uint64_t* g, const uint32_t* bad,
-                                             P1Count& cnt) {
+                                             P1Count& cnt, unsigned valid) {
   Slot* tab = I.table;
   const uint64_t mask = I.table_mask;
   uint64_t idx[N];
@@ -281,6 +291,7 @@ __device__ __forceinline__ void insert_group(InstDev& I, unsigned live, int k, c
   int nf = 0;
 #pragma unroll
   for (int j = 0; j < N; ++j) {
+    if (!((valid >> j) & 1u)) continue;
     int isnew = 0;
     const int r = insert_min(tab, mask, idx[j], cur[j], h[j], l[j], pay_of(k, g[j]), isnew);
     if (r < 0) ++cnt.fail;
@@ -370,7 +381,7 @@ __device__ inline void p1_unary(InstDev& I, const TileSh& P, const uint64_t* sS,
   g[3] = I.base_g + a;
 #pragma unroll
   for (int j = 0; j < 4; ++j) bad[j] &= 1u;
-  insert_group<4>(I, live, P.k, h, l, g, bad, cnt);
+  insert_group<4>(I, live, P.k, h, l, g, bad, cnt, (unsigned)P.mask);
 }
 
 template <int MODE, bool FOUR>
@@ -422,9 +433,9 @@ __device__ inline void p1_binary(InstDev& I, const TileSh& P, const uint64_t* sS
     if (FOUR) {
       key_final<MODE>(kV, h[3], l[3]);
       g[3] = I.base_u[P.j] + b * P.ni + a;
-      insert_group<4>(I, live, P.k, h, l, g, bad, cnt);
+      insert_group<4>(I, live, P.k, h, l, g, bad, cnt, (unsigned)P.mask);
     } else {
-      insert_group<3>(I, live, P.k, h, l, g, bad, cnt);
+      insert_group<3>(I, live, P.k, h, l, g, bad, cnt, (unsigned)P.mask & 7u);
     }
   }
 }
@@ -463,7 +474,7 @@ __device__ inline int reconstruct_to(const InstDev& I, int lvl, uint64_t g, int1
   while (sp >= 0) {
     if (out >= cap) return 0;
     Fr& f = st[sp];
-    if (f.lvl <= 1) {
+    if (f.lvl <= atom_level(I)) {
       rpn[out++] = (int16_t)f.g;
       --sp;
       continue;
