@@ -145,11 +145,11 @@ __device__ void plan_one(InstDev& I) {
       }
       I.grp_prefix[q + 1] = t;
     }
-    for (int q = ng; q < kGroups; ++q) I.grp_prefix[q + 1] = t;
     if (t >= (uint64_t)kP1TileTarget || lg == 0) break;
     --lg;
   }
   I.tq = 1 << lg;
+  for (int q = ng; q < kGroups; ++q) I.grp_prefix[q + 1] = t;
   const uint64_t words = (g + 31) / 32;
   const uint64_t cap = I.table_mask + 1;
   // new keys of this level: at most all candidates; expect ~8x growth
