@@ -62,6 +62,7 @@ struct InstDev {
   uint8_t cost[8];             // operator costs c1..c8 of LTL_BS (p ~ & | X F G U); 0 means 1.
                                // Level k holds the formulas of cost k (unit costs: size k)
   int neg_type;                // 2: ~ applies to propositions only (LTL_BS NegType)
+  int weighted;                // some cost above 1 or neg_type 2 (else the size order's fast paths)
   // ---- buffers (host-owned allocations; pointers may change between levels)
   uint64_t* rows;              // [row_cap][TP]
   uint64_t* origin;            // [row_cap] candidate index within the row's level

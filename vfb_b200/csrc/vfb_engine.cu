@@ -832,6 +832,8 @@ struct Engine {
     // operator costs of the call (vfb_solve_costs), else unit costs
     for (int c = 0; c < 8; ++c) d.cost[c] = (uint8_t)req_cost[c];
     d.neg_type = req_neg;
+    d.weighted = req_neg == 2;
+    for (int c = 0; c < 8; ++c) d.weighted |= req_cost[c] > 1;
     if (atom_level(d) > d.max_size) return VFB_BAD_INPUT;
     d.status = ST_RUNNING;
     d.level = 1;

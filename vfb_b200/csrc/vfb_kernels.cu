@@ -86,6 +86,17 @@ __device__ void plan_one(InstDev& I) {
   // unit costs one unary group and one group per split, as the reference's
   // launches fuse them
   int ng = 0;
+  if (!I.weighted) {
+    // unit costs: one unary group over level k-1, one group per size split
+    I.grp_kind[0] = 0; I.grp_la[0] = (uint8_t)(k - 1); I.grp_lb[0] = 0; I.grp_mask[0] = 0xF;
+    ng = 1;
+    for (int i = 1; 2 * i <= k - 1; ++i, ++ng) {
+      I.grp_kind[ng] = 1;
+      I.grp_la[ng] = (uint8_t)i;
+      I.grp_lb[ng] = (uint8_t)(k - 1 - i);
+      I.grp_mask[ng] = (uint8_t)(i == k - 1 - i ? 7 : 15);
+    }
+  }
   auto unary = [&](int L, int bit) {
     if (L < c1) return;
     for (int q = 0; q < ng; ++q)
@@ -101,11 +112,11 @@ __device__ void plan_one(InstDev& I) {
     I.grp_kind[ng] = 1; I.grp_la[ng] = (uint8_t)la; I.grp_lb[ng] = (uint8_t)lb; I.grp_mask[ng] = (uint8_t)bits;
     ++ng;
   };
-  unary(Ln, 0);
-  unary(k - op_cost(I, OP_X), 1);
-  unary(k - op_cost(I, OP_F), 2);
-  unary(k - op_cost(I, OP_G), 3);
-  {
+  if (I.weighted) unary(Ln, 0);
+  if (I.weighted) unary(k - op_cost(I, OP_X), 1);
+  if (I.weighted) unary(k - op_cost(I, OP_F), 2);
+  if (I.weighted) unary(k - op_cost(I, OP_G), 3);
+  if (I.weighted) {
     const int s3 = k - op_cost(I, OP_AND), s4 = k - op_cost(I, OP_OR), s8 = k - op_cost(I, OP_U);
     const int sums[3] = {s3, s4, s8};
     for (int q = 0; q < 3; ++q) {

@@ -150,10 +150,47 @@ __device__ __forceinline__ void divmod64(uint64_t g, uint64_t n, uint64_t& q, ui
 // costs, LTL_BS.cu:1226-1488 with the operator costs).
 __device__ inline Cand decode(const InstDev& I, int k, uint64_t g) {
   const uint64_t* n = I.lcount;
-  const int c1 = atom_level(I);
   Cand c;
   c.lb = 0;
   c.b = 0;
+  if (!I.weighted) {
+    // unit costs: the size order
+    const uint64_t un = n[k - 1];
+    if (g < un) { c.op = OP_NOT; c.la = k - 1; c.a = g; return c; }
+    g -= un;
+    for (int pass = 0; pass < 2; ++pass) {
+      for (int i = 1; 2 * i <= k - 1; ++i) {
+        const int j = k - 1 - i;
+        const uint64_t cnt = n[i] * n[j];
+        if (g < cnt) {
+          c.op = pass ? OP_OR : OP_AND;
+          c.la = i; c.lb = j;
+          divmod64(g, n[j], c.a, c.b);
+          return c;
+        }
+        g -= cnt;
+      }
+    }
+    for (int op = OP_X; op <= OP_G; ++op) {
+      if (g < un) { c.op = op; c.la = k - 1; c.a = g; return c; }
+      g -= un;
+    }
+    for (int i = 1; i <= k - 2; ++i) {
+      const int j = k - 1 - i;
+      const uint64_t cnt = n[i] * n[j];
+      if (g < cnt) {
+        c.op = OP_U; c.la = i; c.lb = j;
+        divmod64(g, n[j], c.a, c.b);
+        return c;
+      }
+      g -= cnt;
+    }
+    c.op = -1;
+    c.la = 1;
+    c.a = 0;
+    return c;
+  }
+  const int c1 = atom_level(I);
   const int Ln = not_level(I, k);
   if (Ln >= 0) {
     if (g < n[Ln]) { c.op = OP_NOT; c.la = Ln; c.a = g; return c; }
