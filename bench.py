@@ -123,13 +123,22 @@ def _dist():
 
 
 def _allreduce_max(x: float, world: int) -> float:
+    """Maximum over the ranks (the slowest replica's time)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_value(units_per_rank: int, seconds_per_rank: float, world: int) -> float:
+    """Whole-job throughput of N replicas: the units of all ranks (each rank
+    solves the same workload) over the slowest rank's time."""
+    slowest = _allreduce_max(seconds_per_rank, world)
+    return world * units_per_rank / slowest
 
 
 def _barrier(world: int):
@@ -300,6 +309,8 @@ def main():
     _barrier(world)
     dev_total = _allreduce_max(sum(dev_s), world)
     wall_total = _allreduce_max(sum(wall_s), world)
+    value = world * units / dev_total
+    e2e = world * units / wall_total
     answer = r.infix(inst.names)
     eng.close()
 
@@ -334,8 +345,6 @@ def main():
                 "us_per_launch": per_launch_s * 1e6, "launches": nl,
                 "share_of_kernel_time": ms / sum(p[2] for p in prof)}
 
-    value = world * units / dev_total
-    e2e = world * units / wall_total
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * dev_total / args.steps,
