@@ -42,8 +42,11 @@ __device__ inline int insert_min(Slot* tab, uint64_t mask, uint64_t& idx, Key128
       const Key128 old = atomicCAS(reinterpret_cast<Key128*>(tab + idx), Key128{kEmpty, kEmpty},
                                    Key128{h, l});
       if (old.h == kEmpty && old.l == kEmpty) {
+        // this thread published the key: its payload is still the empty word,
+        // so the minimum needs no read first (and its result is not awaited)
         isnew = 1;
-        return claim(tab + idx, pay);
+        atomicMin(&tab[idx].pay, pay);
+        return 1;
       }
       if (old.h == h && old.l == l) return claim(tab + idx, pay);
     }
