@@ -409,13 +409,25 @@ __device__ void ph_table_scan(const BatchDev& B, unsigned bid, unsigned nb) {
     const uint64_t cap = listed ? I.n_newlist : I.table_mask + 1;
     const uint64_t s1 = (s0 + kScanSlots < cap) ? s0 + kScanSlots : cap;
     unsigned long long cnt = 0;
-    for (uint64_t e = s0 + threadIdx.x; e < s1; e += blockDim.x) {
-      const uint64_t sl = listed ? __ldcg(I.wins + e) : e;
-      const unsigned long long pay = __ldcg(&I.table[sl].pay);
-      if ((pay >> kPayShift) == k) {
-        const uint64_t g = pay & kIdxMask;
-        atomicOr(I.bitmap + (g >> 5), 1u << (g & 31));
-        ++cnt;
+    // kScanBatch entries per thread at a time: their list reads, then their
+    // payload reads, are in flight together
+    for (uint64_t e0 = s0 + threadIdx.x; e0 < s1; e0 += (uint64_t)kScanBatch * blockDim.x) {
+      uint64_t sl[kScanBatch];
+      unsigned long long pay[kScanBatch];
+#pragma unroll
+      for (int u = 0; u < kScanBatch; ++u) {
+        const uint64_t e = e0 + (uint64_t)u * blockDim.x;
+        sl[u] = e < s1 ? (listed ? __ldcg(I.wins + e) : e) : ~0ULL;
+      }
+#pragma unroll
+      for (int u = 0; u < kScanBatch; ++u) pay[u] = sl[u] != ~0ULL ? __ldcg(&I.table[sl[u]].pay) : ~0ULL;
+#pragma unroll
+      for (int u = 0; u < kScanBatch; ++u) {
+        if ((pay[u] >> kPayShift) == k) {
+          const uint64_t g = pay[u] & kIdxMask;
+          atomicOr(I.bitmap + (g >> 5), 1u << (g & 31));
+          ++cnt;
+        }
       }
     }
     cnt = warp_sum(cnt);
