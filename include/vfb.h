@@ -95,6 +95,12 @@ typedef struct {
 vfb_status vfb_create(void **ctx, const vfb_opts *opts);
 void vfb_destroy(void *ctx);
 
+/* The cached search (LTLI LTL_BS.cu:1069-1532 in the canonical order of
+ * ltl_nocache).  Buffers grow up to opts->mem_limit_bytes; when a level's
+ * rows cannot be held, that level's candidates are still tested as solutions
+ * without being stored (the reference's onTheFly mode, LTL_BS.cu:331-349):
+ * a solution found there is returned as usual with level_rows[size] = 0,
+ * otherwise the call ends with VFB_LIMIT and the sizes it stored. */
 vfb_status vfb_solve(void *ctx, const vfb_instance *inst, vfb_result *out);
 
 /* Solves n independent instances together; out[i] equals vfb_solve(inst[i]). */

@@ -141,3 +141,31 @@ def test_exact_key_boundary(engine):
     # to 127 (the first relaxed one)
     _check(engine, cases.random_instance(7200, 2, 3, 3, [21] * 6, 7))
     _check(engine, cases.random_instance(7300, 2, 3, 3, [21] * 5 + [22], 7))
+
+
+def test_on_the_fly_level(engine):
+    # a memory budget that cannot hold the solution level's rows: its
+    # candidates are tested without being stored, and the answer is the one
+    # the unbounded search gives (LTL_BS's onTheFly mode)
+    prob = vfb_b200.Problem.from_instance(synth.config_planted())
+    full = engine.solve(prob)
+    assert full.status == vfb_b200.OK
+    hits = 0
+    for mb in [4.0, 3.5, 3.0, 2.75, 2.5, 2.25, 2.0, 1.75, 1.5]:
+        e = vfb_b200.Engine(mem_limit_bytes=int(mb * (1 << 20)))
+        try:
+            r = e.solve(prob)
+        finally:
+            e.close()
+        if r.status == vfb_b200.OK and r.level_rows[-1] == 0:
+            hits += 1
+            assert (r.size, r.rpn, r.solution_index) == (full.size, full.rpn, full.solution_index)
+            assert r.level_rows[:-1] == full.level_rows[:-1]
+            assert r.level_cands == full.level_cands
+        elif r.status == vfb_b200.OK:
+            assert (r.size, r.rpn, r.level_rows) == (full.size, full.rpn, full.level_rows)
+        elif r.status == vfb_b200.LIMIT:
+            assert r.size < full.size and r.level_rows == full.level_rows[:r.size]
+        else:
+            assert r.status == vfb_b200.OOM
+    assert hits >= 1

@@ -34,6 +34,7 @@ enum Status : int {
   ST_NOT_FOUND = 3,
   ST_NEED_MEM = 4,     // a buffer is too small: host grows it and re-runs the level
   ST_ERROR = 5,
+  ST_LIMIT = 6,        // an on-the-fly level held no solution: the search cannot go on
 };
 
 enum NeedBits : int {
@@ -63,6 +64,8 @@ struct InstDev {
                                // Level k holds the formulas of cost k (unit costs: size k)
   int neg_type;                // 2: ~ applies to propositions only (LTL_BS NegType)
   int weighted;                // some cost above 1 or neg_type 2 (else the size order's fast paths)
+  int on_the_fly;              // the level's rows did not fit: its candidates are only tested as
+                               // solutions, nothing is stored (LTL_BS onTheFly, LTL_BS.cu:331-349)
   // ---- buffers (host-owned allocations; pointers may change between levels)
   uint64_t* rows;              // [row_cap][TP]
   uint64_t* origin;            // [row_cap] candidate index within the row's level

@@ -999,7 +999,21 @@ struct Engine {
           const int st = h_status[i].x;
           if (st == ST_RUNNING) running = true;
           if (st == ST_NEED_MEM) {
-            const vfb_status g = grow(H[i], i);
+            vfb_status g = grow(H[i], i);
+            if (g == VFB_OOM && !H[i].d.on_the_fly) {
+              // the level's rows do not fit the budget: test its candidates as
+              // solutions without storing them (LTL_BS onTheFly)
+              InstDev& d = H[i].d;
+              d.on_the_fly = 1;
+              d.status = ST_RUNNING;
+              d.need = 0;
+              d.planned = 0;
+              if (cudaMemcpyAsync(dInst + i, &d, sizeof(InstDev), cudaMemcpyHostToDevice, stream) != cudaSuccess)
+                g = dev_fail(__LINE__);
+              else
+                g = VFB_OK;
+              c_h2d += sizeof(InstDev);
+            }
             if (g != VFB_OK) {
               // this instance stops; the others carry on
               H[i].fail = g;
@@ -1089,6 +1103,8 @@ struct Engine {
         if (d.rpn_len < 1 || rpn_cost(d, d.rpn, d.rpn_len) != d.res_size) r.status = VFB_DEVICE_ERROR;
       } else if (d.status == ST_NOT_FOUND) {
         r.status = VFB_NOT_FOUND;
+      } else if (d.status == ST_LIMIT) {
+        r.status = VFB_LIMIT;   // the on-the-fly level held no solution; sizes are the stored levels
       } else {
         r.status = H[i].fail != VFB_OK ? H[i].fail : (rc != VFB_OK ? rc : VFB_DEVICE_ERROR);
         // the level in progress is not complete: report the finished ones
@@ -1258,6 +1274,8 @@ struct Engine {
       r.solution_index = d.sol_index;
     } else if (d.status == ST_NOT_FOUND) {
       r.status = VFB_NOT_FOUND;
+    } else if (d.status == ST_LIMIT) {
+      r.status = VFB_LIMIT;
     } else {
       r.status = H.fail != VFB_OK ? H.fail : VFB_DEVICE_ERROR;
       if (r.size >= 1 && d.level <= r.size) {
@@ -1368,7 +1386,7 @@ struct Engine {
           cudaMemcpyAsync(&dInst[i].status, &err, sizeof(int), cudaMemcpyHostToDevice, stream);
           fin.push_back(i);
         }
-      } else if (st == ST_FOUND || st == ST_NOT_FOUND || st == ST_ERROR) {
+      } else if (st == ST_FOUND || st == ST_NOT_FOUND || st == ST_ERROR || st == ST_LIMIT) {
         fin.push_back(i);
       }
     }

@@ -161,18 +161,20 @@ __device__ void plan_one(InstDev& I) {
   }
   I.tq = 1 << lg;
   for (int q = ng; q < kGroups; ++q) I.grp_prefix[q + 1] = t;
-  const uint64_t words = (g + 31) / 32;
+  const uint64_t words = I.on_the_fly ? 0 : (g + 31) / 32;
   const uint64_t cap = I.table_mask + 1;
   // new keys of this level: at most all candidates; expect ~8x growth
   const uint64_t grow = 8 * n[k - 1] + 4096;
   const uint64_t est = g < grow ? g : grow;
   int need = 0;
   if (g >= (1ULL << kPayShift)) need |= NEED_LIMIT;
-  if (g > I.promote_above) need |= NEED_PROMOTE;
-  if (words > I.bitmap_words) { need |= NEED_BITMAP; I.need_amount[0] = words; }
-  if (2 * (I.keys + est) > cap) { need |= NEED_TABLE; I.need_amount[1] = 4 * (I.keys + est); }
-  if (I.lstart[k] + est > I.row_cap) { need |= NEED_ROWS; I.need_amount[3] = I.lstart[k] + est; }
-  if (est > I.tent_cap) { need |= NEED_LIST; I.need_amount[2] = est; }
+  if (!I.on_the_fly) {   // an on-the-fly level stores nothing
+    if (g > I.promote_above) need |= NEED_PROMOTE;
+    if (words > I.bitmap_words) { need |= NEED_BITMAP; I.need_amount[0] = words; }
+    if (2 * (I.keys + est) > cap) { need |= NEED_TABLE; I.need_amount[1] = 4 * (I.keys + est); }
+    if (I.lstart[k] + est > I.row_cap) { need |= NEED_ROWS; I.need_amount[3] = I.lstart[k] + est; }
+    if (est > I.tent_cap) { need |= NEED_LIST; I.need_amount[2] = est; }
+  }
   if (need) {
     I.status = ST_NEED_MEM;
     I.need = need;
@@ -180,7 +182,7 @@ __device__ void plan_one(InstDev& I) {
   } else {
     I.plan_tiles = t;
     I.plan_words = words;
-    I.plan_tchunks = (cap + kScanSlots - 1) / kScanSlots;
+    I.plan_tchunks = I.on_the_fly ? 0 : (cap + kScanSlots - 1) / kScanSlots;
     I.planned = k;
     I.p1_done = 0;
     I.p1_step = t;
@@ -285,7 +287,8 @@ __device__ void ph_p1(const BatchDev& B) {
           P.pos[0] = pos0;
           P.pos[1] = pos1;
           // give up early once the table is known to be too small for this level
-          P.skip = (fails != 0) || (4 * (keys + fresh) > 3 * cap);
+          P.otf = __ldcg(&Ip->on_the_fly);
+          P.skip = !P.otf && ((fails != 0) || (4 * (keys + fresh) > 3 * cap));
           P.kind = kind;
           P.mask = gmask;
           if (kind == 0) {
@@ -333,7 +336,9 @@ __device__ void ph_p1(const BatchDev& B) {
       stage_wait();
     }
     __syncthreads();
-    if (!P.skip) {
+    if (!P.skip && P.otf) {
+      p1_solutions(I, P, sS, sp, sQ, cnt);
+    } else if (!P.skip) {
       const bool four = P.kind == 1 && (P.mask & 8);
       switch (P.mode) {
         case KEY_HASH:
@@ -446,7 +451,7 @@ __device__ void ph_table_scan(const BatchDev& B, unsigned bid, unsigned nb) {
   const unsigned long long nw = ((unsigned long long)nb * blockDim.x) >> 5;
   for (unsigned long long b = gw; b < (unsigned long long)B.ninst; b += nw) {
     InstDev& I = B.inst[b];
-    if (I.status != ST_RUNNING || I.best_cand == ~0ULL || !I.p1_tail) continue;
+    if (I.status != ST_RUNNING || I.best_cand == ~0ULL || !I.p1_tail || I.on_the_fly) continue;
     const int k = I.level;
     const uint64_t g = I.best_cand;
     const Cand cd = decode(I, k, g);
@@ -717,6 +722,28 @@ __global__ void k_emit_rows(BatchDev* Bp) {
 // the formula is rebuilt from the cache (LTL_BS.cu:561-705).
 __device__ void finish_one(InstDev& I) {
   const int k = I.level;
+  if (I.on_the_fly) {
+    // nothing of the level was stored: its first solving candidate, if any,
+    // is the answer (it owns its word: no earlier candidate or level has it)
+    I.lcount[k] = 0;
+    I.built_cands = I.cands;
+    I.built_wins = 0;
+    I.built_scanned = 0;
+    I.built_sol_known = 1;
+    if (I.best_cand != ~0ULL) {
+      const uint64_t g = I.best_cand;
+      I.lcands[k] = g + 1;
+      I.sol_index = g;
+      I.res_size = k;
+      I.status = ST_FOUND;
+      reconstruct(I, k, g);
+    } else {
+      I.lcands[k] = I.cands;
+      I.res_size = k - 1;
+      I.status = ST_LIMIT;
+    }
+    return;
+  }
   I.built_cands = I.cands;
   I.built_wins = I.n_wins;
   I.built_scanned = (I.attempt == 1 && I.n_newlist <= I.tent_cap) ? I.n_newlist : I.table_mask + 1;

@@ -281,6 +281,7 @@ struct TileSh {
   unsigned long long tile;
   int inst, grp, k, T, TP, half, stride, mode, skip;
   int kind, mask;   // operand group: 0 unary / 1 binary; the operators it evaluates
+  int otf;          // on-the-fly level: solution test only, nothing inserted
   uint64_t s0, q0, nS, nQ, ni, nj;
   int si, qi;   // levels of the stream / staged operand
   int qleft;    // staged operand is the left operand of & | and of U(i->j)
@@ -477,6 +478,51 @@ __device__ inline void p1_binary(InstDev& I, const TileSh& P, const uint64_t* sS
     } else {
       insert_group<3>(I, live, P.k, h, l, g, bad, cnt, (unsigned)P.mask & 7u);
     }
+  }
+}
+
+// On-the-fly level (nothing stored): the tile's candidates get the solution
+// test alone, step 0 of every trace against its label; no key, no insert.
+__device__ inline void p1_solutions(InstDev& I, const TileSh& P, const uint64_t* sS, int sp, const uint64_t* sQ,
+                                    P1Count& cnt) {
+  const uint64_t s = P.s0 + threadIdx.x;
+  if (s >= P.nS) return;
+  const uint64_t* srow = sS + threadIdx.x * sp;
+  if (P.kind == 0) {
+    uint32_t bad[4] = {0, 0, 0, 0};
+    for (int t = 0; t < P.T; ++t) {
+      const uint64_t w = srow[t], lm = len_mask(P.len[t]);
+      const uint32_t pb = (uint32_t)pos_bit(P, t);
+      bad[0] |= lo32(~w & lm) ^ pb;
+      bad[1] |= lo32(w >> 1) ^ pb;
+      bad[2] |= lo32(w_fin(w)) ^ pb;
+      bad[3] |= lo32(w_glob(w, lm)) ^ pb;
+    }
+    const uint64_t g[4] = {I.base_not + s, I.base_x + s, I.base_f + s, I.base_g + s};
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (((P.mask >> j) & 1) && !(bad[j] & 1u) && g[j] < cnt.sol) cnt.sol = g[j];
+    return;
+  }
+  const int nq = (int)((P.nQ - P.q0) < (uint64_t)P.tq ? (P.nQ - P.q0) : (uint64_t)P.tq);
+  for (int q = 0; q < nq; ++q) {
+    const uint64_t* qrow = sQ + q * P.TP;
+    uint32_t bad[4] = {0, 0, 0, 0};
+    for (int t = 0; t < P.T; ++t) {
+      const uint64_t qw = qrow[t], sw = srow[t];
+      const uint64_t la = P.qleft ? qw : sw, lb = P.qleft ? sw : qw;
+      const uint32_t pb = (uint32_t)pos_bit(P, t);
+      bad[0] |= lo32(la & lb) ^ pb;
+      bad[1] |= lo32(la | lb) ^ pb;
+      bad[2] |= lo32(w_until(la, lb)) ^ pb;
+      bad[3] |= lo32(w_until(lb, la)) ^ pb;
+    }
+    const uint64_t a = P.qleft ? P.q0 + q : s, b = P.qleft ? s : P.q0 + q;
+    const uint64_t ab = a * P.nj + b;
+    const uint64_t g[4] = {I.base_and[P.i] + ab, I.base_or[P.i] + ab, I.base_u[P.i] + ab, I.base_u[P.j] + b * P.ni + a};
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (((P.mask >> j) & 1) && !(bad[j] & 1u) && g[j] < cnt.sol) cnt.sol = g[j];
   }
 }
 
