@@ -208,6 +208,40 @@ typedef struct {
 int vfb_profile_read(void *ctx, vfb_kernel_stat *out, int cap);
 void vfb_profile_reset(void *ctx);
 
+/* Launch shape of the candidate kernel (k_p1) per level band (no counterpart
+ * in the reference, whose processOperator launches use fixed block sizes,
+ * LTL_BS.cu:1284-1305).  Band b holds the levels of 4^b .. 4^(b+1)-1
+ * candidates, the last band every larger level.  A tile is 128 rows of one
+ * operand level against `rows` staged rows of the other; small levels are cut
+ * into shorter tiles until they have 2^tiles_log2 of them; `blocks` CTAs take
+ * the tiles.  Zero in a field selects the built-in choice (rows 16,
+ * tiles_log2 12, every resident CTA).  Results never depend on the shape. */
+#define VFB_TUNE_BANDS 16
+typedef struct {
+  uint8_t rows[VFB_TUNE_BANDS];         /* staged rows per tile: 1, 2, 4, .. 32 */
+  uint8_t tiles_log2[VFB_TUNE_BANDS];   /* tile count to reach by shorter tiles, log2 (1..40) */
+  uint16_t blocks[VFB_TUNE_BANDS];      /* CTAs of the level's launch */
+  float ms[VFB_TUNE_BANDS];             /* vfb_autotune: k_p1 time of the chosen shape summed
+                                           over the sample's levels in the band (0: none) */
+  float ms_default[VFB_TUNE_BANDS];     /* vfb_autotune: the same with the built-in shape */
+  uint32_t levels[VFB_TUNE_BANDS];      /* vfb_autotune: the sample's levels in the band */
+} vfb_tune;
+
+/* The shape every later solve, batch and served request of ctx uses
+ * (NULL: the built-in shape everywhere). */
+vfb_status vfb_tune_set(void *ctx, const vfb_tune *tune);
+vfb_status vfb_tune_get(void *ctx, vfb_tune *tune);
+
+/* Autotuner: solves the n sample instances once per candidate shape (staged
+ * rows 4/8/16/32 x tile targets 2^8/2^10/2^12/2^14 x every resident CTA or one
+ * per SM), `reps` times each (>= 1), timing k_p1 at every level with CUDA events;
+ * each band takes the shape with the least time over the sample's levels in
+ * that band (bands without a level keep the built-in shape).  The result is
+ * installed in ctx (as vfb_tune_set) and written to *out when out is not
+ * NULL.  Every sample solve must return the same result under every shape,
+ * else VFB_DEVICE_ERROR. */
+vfb_status vfb_autotune(void *ctx, const vfb_instance *sample, int n, int reps, vfb_tune *out);
+
 /* Seeded synthetic instance (no counterpart in the reference, which ships no
  * benchmark inputs): rejection-samples n_pos + n_neg traces with lengths
  * uniform in [len_lo, len_hi] and i.i.d. Bernoulli(p) bits, labelled by a

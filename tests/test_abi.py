@@ -36,6 +36,23 @@ def test_python_binding_lists_all_exports():
     assert set(vfb_b200.EXPORTS) <= _declared_symbols()
 
 
+def test_struct_layouts_match_header(tmp_path):
+    # sizes and field offsets of the ctypes mirrors equal the C compiler's
+    src = tmp_path / "layout.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "vfb.h"\n'
+        'int main(void) {\n'
+        '  printf("%zu %zu %zu %zu %zu\\n", sizeof(vfb_tune), offsetof(vfb_tune, blocks),\n'
+        '         offsetof(vfb_tune, ms), offsetof(vfb_tune, levels), sizeof(vfb_result));\n'
+        '  return 0;\n}\n')
+    exe = tmp_path / "layout"
+    subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)])
+    got = [int(x) for x in subprocess.check_output([str(exe)], text=True).split()]
+    T = vfb_b200._Tune
+    assert got == [ctypes.sizeof(T), T.blocks.offset, T.ms.offset, T.levels.offset,
+                   ctypes.sizeof(vfb_b200._Result)]
+
+
 def test_status_strings():
     lib = vfb_b200.load_library()
     assert lib.vfb_status_str(0) == b"ok"

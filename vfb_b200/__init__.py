@@ -65,6 +65,19 @@ class _KernelStat(ctypes.Structure):
                 ("ms", ctypes.c_double), ("bytes", ctypes.c_double)]
 
 
+TUNE_BANDS = 16
+
+
+class _Tune(ctypes.Structure):
+    _fields_ = [("rows", ctypes.c_uint8 * TUNE_BANDS), ("tiles_log2", ctypes.c_uint8 * TUNE_BANDS),
+                ("blocks", ctypes.c_uint16 * TUNE_BANDS), ("ms", ctypes.c_float * TUNE_BANDS),
+                ("ms_default", ctypes.c_float * TUNE_BANDS), ("levels", ctypes.c_uint32 * TUNE_BANDS)]
+
+
+def _tune_dict(t: _Tune) -> dict:
+    return {f: list(getattr(t, f)) for f, _ in _Tune._fields_}
+
+
 class _JsonProblem(ctypes.Structure):
     _fields_ = [("inst", _Instance), ("max_length_traces", ctypes.c_int),
                 ("names", ctypes.POINTER(ctypes.c_char_p))]
@@ -74,7 +87,8 @@ EXPORTS = ["vfb_create", "vfb_destroy", "vfb_solve", "vfb_batch_solve", "vfb_sta
            "vfb_read_json", "vfb_json_free", "vfb_format_infix", "vfb_profile_read",
            "vfb_profile_reset", "vfb_solve_noalloc", "vfb_synth_planted", "vfb_serve_open",
            "vfb_serve_limits", "vfb_serve_submit", "vfb_serve_step", "vfb_serve_close",
-           "vfb_solve_exhaustive", "vfb_solve_bs", "vfb_solve_costs"]
+           "vfb_solve_exhaustive", "vfb_solve_bs", "vfb_solve_costs", "vfb_tune_set",
+           "vfb_tune_get", "vfb_autotune"]
 
 _lib = None
 
@@ -135,6 +149,13 @@ def load_library():
     lib.vfb_serve_step.restype = ctypes.c_int
     lib.vfb_serve_close.argtypes = [ctypes.c_void_p]
     lib.vfb_serve_close.restype = None
+    lib.vfb_tune_set.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Tune)]
+    lib.vfb_tune_set.restype = ctypes.c_int
+    lib.vfb_tune_get.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Tune)]
+    lib.vfb_tune_get.restype = ctypes.c_int
+    lib.vfb_autotune.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Instance), ctypes.c_int, ctypes.c_int,
+                                 ctypes.POINTER(_Tune)]
+    lib.vfb_autotune.restype = ctypes.c_int
     _lib = lib
     return lib
 
@@ -307,6 +328,42 @@ class Engine:
         self._lib.vfb_solve_exhaustive(self._ctx, ctypes.byref(inst), ctypes.byref(res))
         del keep
         return _result(res)
+
+    # ---- k_p1 launch shape per level band
+    def autotune(self, probs: list, reps: int = 2) -> dict:
+        """Time k_p1 over the sample under each candidate shape and install the
+        fastest per level band; returns the table (vfb_tune fields as lists)."""
+        n = len(probs)
+        arr = (_Instance * n)()
+        keep = []
+        for i, p in enumerate(probs):
+            s, k = p._cstruct()
+            arr[i] = s
+            keep.append(k)
+        t = _Tune()
+        rc = self._lib.vfb_autotune(self._ctx, arr, n, reps, ctypes.byref(t))
+        del keep
+        if rc != OK:
+            raise VfbError(f"vfb_autotune failed: {STATUS_NAMES[rc]}")
+        return _tune_dict(t)
+
+    def set_tune(self, table) -> None:
+        """Install a shape table (dict with rows / tiles_log2 / blocks lists; None: built-in)."""
+        if table is None:
+            rc = self._lib.vfb_tune_set(self._ctx, None)
+        else:
+            t = _Tune()
+            for f, _ in _Tune._fields_:
+                if f in table:
+                    getattr(t, f)[:] = list(table[f])
+            rc = self._lib.vfb_tune_set(self._ctx, ctypes.byref(t))
+        if rc != OK:
+            raise VfbError(f"vfb_tune_set failed: {STATUS_NAMES[rc]}")
+
+    def get_tune(self) -> dict:
+        t = _Tune()
+        self._lib.vfb_tune_get(self._ctx, ctypes.byref(t))
+        return _tune_dict(t)
 
     # ---- serving (continuous batching)
     def serve_limits(self, budget_frac: float = 0.8, request_bytes: int = 0,

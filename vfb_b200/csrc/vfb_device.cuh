@@ -19,7 +19,11 @@ constexpr int kMaxSplits = 16;        // floor((32-1)/2)
 constexpr int kGroups = 64;
 constexpr int kTS = 128;              // stream rows per P1 tile (= threads per CTA)
 constexpr int kTQ = 32;               // staged rows per P1 tile (maximum)
-constexpr int kP1TileTarget = 1024;   // shrink the staged height until a level has this many tiles
+constexpr int kTQDefault = 16;        // staged rows per P1 tile unless the tune table says otherwise
+constexpr int kP1TileTarget = 4096;   // shrink the staged height until a level has this many tiles
+// P1 launch shape per level band (tuned by the host): band b holds the levels
+// of 4^b to 4^(b+1)-1 candidates, the last band every larger level
+constexpr int kTuneBands = 16;
 constexpr int kMaxProbes = 4096;      // bounded linear probing
 constexpr uint64_t kEmpty = ~0ULL;
 constexpr int kPayShift = 58;         // payload = level << 58 | candidate index
@@ -51,6 +55,13 @@ struct __align__(16) Key128 {
   unsigned long long h, l;
 };
 
+// Tuning band of a level of `cands` candidates: floor(log4(cands)), clamped.
+__host__ __device__ inline int tune_band(unsigned long long cands) {
+  int b = 0;
+  while (b < kTuneBands - 1 && (cands >> (2 * b + 2)) != 0) ++b;
+  return b;
+}
+
 // Per-instance device state.  Kernels read everything they need from here,
 // so one captured launch sequence serves every level and every batch.
 struct InstDev {
@@ -59,6 +70,12 @@ struct InstDev {
   uint8_t len[kMaxTraces];
   uint8_t off[kMaxTraces];     // bit offset of the trace's key field (<=126)
   uint8_t width[kMaxTraces];   // key field width (0 when past bit 126)
+  // P1 launch shape by level band (tune_band); 0 everywhere = the built-in
+  // choice: staged rows at most tune_rows (a power of two, 0: kTQDefault), at least
+  // 2^tune_tiles tiles while the staged height can shrink (0: kP1TileTarget),
+  // tune_blocks CTAs (0: every resident CTA)
+  uint8_t tune_rows[kTuneBands], tune_tiles[kTuneBands];
+  uint16_t tune_blocks[kTuneBands];
   uint64_t posmask[2];         // bit i: trace i is positive
   uint8_t cost[8];             // operator costs c1..c8 of LTL_BS (p ~ & | X F G U); 0 means 1.
                                // Level k holds the formulas of cost k (unit costs: size k)
@@ -95,7 +112,7 @@ struct InstDev {
   uint8_t grp_kind[kGroups], grp_mask[kGroups], grp_la[kGroups], grp_lb[kGroups];
   int ngroups;
   int tq;                      // staged rows per P1 tile at this level (1..kTQ)
-  int pad1;
+  int p1_blocks;               // P1 CTAs this level asks for (0: every resident CTA)
   unsigned long long promote_above;  // candidates per level above which the instance
                                      // leaves the cluster solver (~0: never)
   // per-level counters

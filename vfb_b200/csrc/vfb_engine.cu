@@ -58,6 +58,7 @@ const char* const kNames[KP_N] = {"k_advance", "k_p1", "k_table_scan", "k_compac
 // one level (the trailing k_advance finishes it and plans the next).
 const int kStepSeq[] = {KP_ADVANCE, KP_P1, KP_TSCAN, KP_COMPACT, KP_EMIT, KP_ADVANCE};
 constexpr int kStepLen = sizeof(kStepSeq) / sizeof(int);
+constexpr int kStepP1 = 1;    // position of k_p1 in kStepSeq
 constexpr int kBodyLen = 5;   // kernels of one level inside the device-side loop
 constexpr unsigned kMaxLoop = 4 * kMaxSize;
 // serving: P1 candidates of one request per step (a larger level takes
@@ -124,6 +125,14 @@ struct Engine {
   cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr;
   cudaEvent_t ev_k[kStepLen + 1] = {};
   Prof prof[KP_N];
+
+  // P1 launch shape by level band (zero fields: built-in), copied into every
+  // prepared instance
+  vfb_tune tune{};
+  // autotuner: k_p1 milliseconds and levels per band of the solves running
+  // under it (profile_step adds to them when set)
+  double* tune_ms = nullptr;
+  uint32_t* tune_levels = nullptr;
 
   ~Engine() { release(); }
 
@@ -302,7 +311,7 @@ struct Engine {
       WS_ALLOC(win_prefix, pre)
       WS_ALLOC(chunk_cnt, std::max<uint64_t>(cc, 1) * sizeof(unsigned int))
       WS_ALLOC(chunk_base, std::max<uint64_t>(cc, 1) * sizeof(unsigned long long))
-      WS_ALLOC(tickets, 4 * sizeof(unsigned long long))
+      WS_ALLOC(tickets, kTickets * sizeof(unsigned long long))
       WS_ALLOC(status_out, (size_t)nc * sizeof(int2))
       WS_ALLOC(loop_iter, sizeof(unsigned long long))
       WS_ALLOC(ctl, 4 * sizeof(unsigned int))
@@ -542,7 +551,7 @@ struct Engine {
         b.chunk_prefix = (unsigned long long*)take(16);
         b.tscan_prefix = (unsigned long long*)take(16);
         b.win_prefix = (unsigned long long*)take(16);
-        b.tickets = (unsigned long long*)take(32);
+        b.tickets = (unsigned long long*)take(kTickets * sizeof(unsigned long long));
         b.status_out = (int2*)take(16);
         b.loop_iter = (unsigned long long*)take(8);
         b.chunk_cnt = (unsigned int*)take(chunks * 4);
@@ -794,6 +803,11 @@ struct Engine {
     d.T = T;
     d.TP = T + (T & 1);
     d.A = A;
+    for (int b = 0; b < kTuneBands; ++b) {
+      d.tune_rows[b] = tune.rows[b];
+      d.tune_tiles[b] = tune.tiles_log2[b];
+      d.tune_blocks[b] = tune.blocks[b];
+    }
     d.npos = in.num_pos;
     d.max_size = in.max_size;
     d.lensum = S;
@@ -900,6 +914,17 @@ struct Engine {
     }
     std::vector<InstDev> recs(n);
     cudaMemcpy(recs.data(), dInst, (size_t)n * sizeof(InstDev), cudaMemcpyDeviceToHost);
+    if (tune_ms) {
+      // a step that built a level (not one that stopped for memory): its
+      // k_p1 time goes to the band of the level's candidate count
+      for (int i = 0; i < n; ++i) {
+        const InstDev& d = recs[i];
+        if (!H[i].active || d.status == ST_NEED_MEM || d.built_cands == 0) continue;
+        const int b = tune_band(d.built_cands);
+        tune_ms[b] += ms[kStepP1];
+        tune_levels[b] += 1;
+      }
+    }
     for (int i = 0; i < n; ++i) {
       const InstDev& d = recs[i];
       const int k = d.res_size;
@@ -1831,6 +1856,117 @@ struct Engine {
     return r.status = (kfit < K) ? VFB_LIMIT : VFB_NOT_FOUND;
   }
 
+  // ------------------------------------------------------------ autotuner
+  vfb_status tune_set(const vfb_tune* t) {
+    if (!t) {
+      tune = vfb_tune{};
+      return VFB_OK;
+    }
+    for (int b = 0; b < kTuneBands; ++b) {
+      const int r = t->rows[b];
+      if (r > kTQ || (r & (r - 1)) != 0) return VFB_BAD_INPUT;
+      if (t->tiles_log2[b] > 40) return VFB_BAD_INPUT;
+    }
+    tune = *t;
+    return VFB_OK;
+  }
+
+  static bool same_result(const vfb_result& a, const vfb_result& b) {
+    if (a.status != b.status || a.size != b.size || a.rpn_len != b.rpn_len ||
+        a.solution_index != b.solution_index || a.total_rows != b.total_rows)
+      return false;
+    for (int i = 0; i < a.rpn_len && i < VFB_MAX_SIZE; ++i)
+      if (a.rpn[i] != b.rpn[i]) return false;
+    for (int k = 0; k <= VFB_MAX_SIZE; ++k)
+      if (a.level_rows[k] != b.level_rows[k] || a.level_cands[k] != b.level_cands[k]) return false;
+    return true;
+  }
+
+  // Solves the sample under each candidate shape with every kernel of the
+  // level step timed; per band, the shape with the least k_p1 time wins.
+  vfb_status autotune(const vfb_instance* sample, int n, int reps, vfb_tune* out) {
+    if (!sample || n <= 0 || reps < 1) return VFB_BAD_INPUT;
+    struct Shape { uint8_t rows, tiles; uint16_t blocks; };
+    std::vector<Shape> shapes;
+    for (int r : {4, 8, 16, 32})
+      for (int t : {8, 10, 12, 14})
+        for (int b : {0, sms}) shapes.push_back(Shape{(uint8_t)r, (uint8_t)t, (uint16_t)b});
+    const int sv_profile = profile;
+    const bool sv_loop = use_loop, sv_coop = use_coop, sv_cluster = use_cluster;
+    Prof sv_prof[KP_N];
+    std::memcpy(sv_prof, prof, sizeof(prof));
+    profile = 1;
+    use_loop = use_coop = use_cluster = false;
+    if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
+    tune = vfb_tune{};
+    vfb_status rc = VFB_OK;
+    // reference results (and buffers at their final sizes) under the built-in shape
+    std::vector<vfb_result> want(n);
+    for (int i = 0; i < n && rc == VFB_OK; ++i) {
+      const vfb_status s = batch(&sample[i], 1, &want[i]);
+      if (s != VFB_OK) rc = s;
+    }
+    const size_t ns = shapes.size();
+    std::vector<double> best(ns * kTuneBands, 0.0);
+    std::vector<uint32_t> lv(ns * kTuneBands, 0);
+    for (size_t c = 0; c < ns && rc == VFB_OK; ++c) {
+      for (int b = 0; b < kTuneBands; ++b) {
+        tune.rows[b] = shapes[c].rows;
+        tune.tiles_log2[b] = shapes[c].tiles;
+        tune.blocks[b] = shapes[c].blocks;
+      }
+      for (int r = 0; r < reps && rc == VFB_OK; ++r) {
+        double acc[kTuneBands] = {};
+        uint32_t lev[kTuneBands] = {};
+        tune_ms = acc;
+        tune_levels = lev;
+        for (int i = 0; i < n && rc == VFB_OK; ++i) {
+          vfb_result got;
+          const vfb_status s = batch(&sample[i], 1, &got);
+          if (s != VFB_OK) rc = s;
+          else if (!same_result(got, want[i])) rc = dev_fail(__LINE__);
+        }
+        tune_ms = nullptr;
+        tune_levels = nullptr;
+        for (int b = 0; b < kTuneBands; ++b) {
+          double& m = best[c * kTuneBands + b];
+          if (r == 0 || acc[b] < m) m = acc[b];
+          lv[c * kTuneBands + b] = lev[b];
+        }
+      }
+    }
+    vfb_tune res{};
+    if (rc == VFB_OK) {
+      size_t dflt = 0;
+      for (size_t c = 0; c < ns; ++c)
+        if (shapes[c].rows == kTQDefault && (1 << shapes[c].tiles) == kP1TileTarget && shapes[c].blocks == 0)
+          dflt = c;
+      for (int b = 0; b < kTuneBands; ++b) {
+        if (lv[dflt * kTuneBands + b] == 0) continue;
+        size_t w = dflt;
+        for (size_t c = 0; c < ns; ++c)
+          if (best[c * kTuneBands + b] < best[w * kTuneBands + b]) w = c;
+        if (w != dflt) {
+          res.rows[b] = shapes[w].rows;
+          res.tiles_log2[b] = shapes[w].tiles;
+          res.blocks[b] = shapes[w].blocks;
+        }
+        res.ms[b] = (float)best[w * kTuneBands + b];
+        res.ms_default[b] = (float)best[dflt * kTuneBands + b];
+        res.levels[b] = lv[dflt * kTuneBands + b];
+      }
+    }
+    profile = sv_profile;
+    use_loop = sv_loop;
+    use_coop = sv_coop;
+    use_cluster = sv_cluster;
+    std::memcpy(prof, sv_prof, sizeof(prof));
+    if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
+    tune = rc == VFB_OK ? res : vfb_tune{};
+    if (out && rc == VFB_OK) *out = res;
+    return rc;
+  }
+
   int profile_read(vfb_kernel_stat* outp, int cap) {
     int m = 0;
     for (int k = 0; k < KP_N && m < cap; ++k) {
@@ -1944,6 +2080,22 @@ vfb_status vfb_serve_step(void* ctx, vfb_served* done, int cap, int* ndone, int*
 
 void vfb_serve_close(void* ctx) {
   if (ctx) static_cast<Engine*>(ctx)->serve_close();
+}
+
+vfb_status vfb_tune_set(void* ctx, const vfb_tune* tune) {
+  if (!ctx) return VFB_BAD_INPUT;
+  return static_cast<Engine*>(ctx)->tune_set(tune);
+}
+
+vfb_status vfb_tune_get(void* ctx, vfb_tune* tune) {
+  if (!ctx || !tune) return VFB_BAD_INPUT;
+  *tune = static_cast<Engine*>(ctx)->tune;
+  return VFB_OK;
+}
+
+vfb_status vfb_autotune(void* ctx, const vfb_instance* sample, int n, int reps, vfb_tune* out) {
+  if (!ctx) return VFB_BAD_INPUT;
+  return static_cast<Engine*>(ctx)->autotune(sample, n, reps, out);
 }
 
 int vfb_profile_read(void* ctx, vfb_kernel_stat* out, int cap) {

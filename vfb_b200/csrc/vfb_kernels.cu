@@ -136,10 +136,16 @@ __device__ void plan_one(InstDev& I) {
   I.ngroups = ng;
   // P1 tiling: kTS stream rows x tq staged rows per tile; small levels get
   // shorter tiles so that they still spread over every SM
-  // (tq is a power of two: tile counts by shifts, not 64-bit divisions)
+  // (tq is a power of two: tile counts by shifts, not 64-bit divisions).
+  // The level's band of the tune table bounds the staged height, sets the
+  // tile count to reach and the CTAs to launch.
+  const int band = tune_band(g);
+  const int rows_cap = I.tune_rows[band] ? (I.tune_rows[band] < kTQ ? I.tune_rows[band] : kTQ) : kTQDefault;
+  const uint64_t target = I.tune_tiles[band] ? 1ULL << I.tune_tiles[band] : (uint64_t)kP1TileTarget;
+  I.p1_blocks = I.tune_blocks[band];
   uint64_t t = 0;
   int lg = 0;
-  while ((1 << (lg + 1)) <= kTQ) ++lg;
+  while ((1 << (lg + 1)) <= rows_cap) ++lg;
   for (;;) {
     t = 0;
     I.grp_prefix[0] = 0;
@@ -156,7 +162,7 @@ __device__ void plan_one(InstDev& I) {
       }
       I.grp_prefix[q + 1] = t;
     }
-    if (t >= (uint64_t)kP1TileTarget || lg == 0) break;
+    if (t >= target || lg == 0) break;
     --lg;
   }
   I.tq = 1 << lg;
@@ -224,7 +230,7 @@ __device__ void ph_plan_prefix(const BatchDev& B) {
     B.chunk_prefix[b + 1] += B.chunk_prefix[b];
     B.tscan_prefix[b + 1] += B.tscan_prefix[b];
   }
-  for (int i = 0; i < 4; ++i) B.tickets[i] = 0;
+  for (int i = 0; i < kTickets; ++i) B.tickets[i] = 0;
 }
 
 __global__ void k_plan(BatchDev* Bp) {
@@ -392,6 +398,8 @@ __global__ void __launch_bounds__(kTS) k_p1(BatchDev* Bp) {
   step_entry();
   const BatchDev B = *Bp;
   if (blockIdx.x >= B.p1_prefix[B.ninst]) return;   // more CTAs than tiles: no ticket needed
+  const unsigned long long cap = B.tickets[kTicketP1Blocks];
+  if (cap && blockIdx.x >= cap) return;               // the tuned CTA count of this step
   ph_p1(B);
 }
 
@@ -793,6 +801,7 @@ __global__ void k_finish(BatchDev* Bp) {
 __global__ void __launch_bounds__(1024) k_advance(BatchDev* Bp, cudaGraphConditionalHandle handle, int built,
                                                   int loop, unsigned int max_iter) {
   __shared__ int s_run, s_need;
+  __shared__ unsigned s_blocks;
   __shared__ unsigned long long s_w[32];
   __shared__ unsigned long long s_carry[3];
   step_entry();
@@ -800,10 +809,12 @@ __global__ void __launch_bounds__(1024) k_advance(BatchDev* Bp, cudaGraphConditi
   if (threadIdx.x == 0) {
     s_run = 0;
     s_need = 0;
+    s_blocks = 0;
     s_carry[0] = s_carry[1] = s_carry[2] = 0;
   }
   __syncthreads();
   int run = 0, need = 0;
+  unsigned blocks = 0;   // CTAs the step's P1 asks for (~0u: every resident CTA)
   for (int base = 0; base < B.ninst; base += blockDim.x) {
     const int b = base + threadIdx.x;
     unsigned long long tiles = 0, chunks = 0, tchunks = 0;
@@ -825,6 +836,8 @@ __global__ void __launch_bounds__(1024) k_advance(BatchDev* Bp, cudaGraphConditi
         I.p1_step = step;
         I.p1_tail = step == left;
         tiles = step;
+        const unsigned want = I.p1_blocks ? (unsigned)I.p1_blocks : ~0u;
+        blocks = want > blocks ? want : blocks;
         if (I.p1_tail) {
           chunks = (I.plan_words + kCompactWords - 1) / kCompactWords;
           tchunks = I.plan_tchunks;
@@ -852,11 +865,14 @@ __global__ void __launch_bounds__(1024) k_advance(BatchDev* Bp, cudaGraphConditi
   }
   if (run) atomicOr(&s_run, 1);
   if (need) atomicOr(&s_need, 1);
+  if (blocks) atomicMax(&s_blocks, blocks);
+  __syncthreads();
   if (threadIdx.x == 0) {
     B.p1_prefix[0] = 0;
     B.chunk_prefix[0] = 0;
     B.tscan_prefix[0] = 0;
     for (int i = 0; i < 4; ++i) B.tickets[i] = 0;
+    B.tickets[kTicketP1Blocks] = s_blocks == ~0u ? 0 : s_blocks;
   }
   __syncthreads();
   const unsigned long long nchunks = s_carry[1];

@@ -11,6 +11,8 @@ constexpr int kScanSlots = 8192;      // hash-set slots per table-scan chunk
 constexpr int kScanBatch = 8;         // table-scan entries a thread reads at a time
 constexpr int kCompactWords = 512;    // owner-bitmap words per k_compact chunk (16384 candidates)
 constexpr int kCompactThreads = 256;  // threads per k_compact CTA (two bitmap words each)
+constexpr int kTickets = 8;            // words of BatchDev::tickets
+constexpr int kTicketP1Blocks = 4;     // tickets[4]: CTAs the step's k_p1 runs (0: all), set by k_advance
 constexpr int kEmitGroup = 4;         // owners per warp step of k_emit
 
 // Global batch descriptor, resident in device memory so that buffer growth
@@ -28,7 +30,8 @@ struct BatchDev {
   unsigned long long* chunk_base;       // [chunk_cap] chunk offsets (k_chunk_*), or the
                                         // look-back states of k_compact (flag << 62 | count)
   unsigned long long chunk_cap;
-  unsigned long long* tickets;          // [4]: P1 work ticket, scan done counter
+  unsigned long long* tickets;          // [kTickets]: P1 work ticket, scan done counter,
+                                        // compaction ticket, (unused), P1 CTAs of the step
   int2* status_out;                     // [ninst] (status, need) mirror for the host
   unsigned long long* loop_iter;        // level steps run by the current device-side loop
   unsigned int* ctl;                    // persistent solver: [0] barrier arrivals, [1] barrier

@@ -177,7 +177,7 @@ extern "C" vfb_status vfb_solve_noalloc(const vfb_instance* inst, vfb_result* ou
   hB.chunk_prefix = cv.take<unsigned long long>(2);
   hB.tscan_prefix = cv.take<unsigned long long>(2);
   hB.win_prefix = cv.take<unsigned long long>(2);
-  hB.tickets = cv.take<unsigned long long>(4);
+  hB.tickets = cv.take<unsigned long long>(kTickets);
   hB.status_out = cv.take<int2>(1);
   hB.loop_iter = cv.take<unsigned long long>(1);
   hB.chunk_cap = kNaWords / kChunkWords + 2;
