@@ -175,6 +175,16 @@ def run_reference(args, inst):
     print(json.dumps(line), flush=True)
 
 
+def _tune_summary(table: dict, sample: str) -> dict:
+    """The autotuned k_p1 shape of the bands the sample's levels fell in:
+    band -> [staged rows, log2 tile target, CTAs] (0: built-in), and the
+    sample's k_p1 time under it against the built-in shape."""
+    bands = {b: [table["rows"][b], table["tiles_log2"][b], table["blocks"][b]]
+             for b in range(len(table["levels"])) if table["levels"][b]}
+    return {"sample": sample, "bands": bands,
+            "p1_ms_tuned": round(sum(table["ms"]), 4), "p1_ms_builtin": round(sum(table["ms_default"]), 4)}
+
+
 def batched(local: int, flush, count: int = 256, reps: int = 3):
     """The mixed batch (seed 3): one vfb_batch_solve of every instance against
     one vfb_solve per instance on the same engine, both warm (device timeline
@@ -184,6 +194,7 @@ def batched(local: int, flush, count: int = 256, reps: int = 3):
     from vfb_b200 import synth
     probs = [vfb_b200.Problem.from_instance(i) for i in synth.config_batch(count=count)]
     eng = vfb_b200.Engine(device=local)
+    tuned = _tune_summary(eng.autotune(probs[:16], reps=2), "the batch's first 16 instances, solved one by one")
     key = lambda r: (r.status, r.size, r.rpn, r.level_rows, r.level_cands)  # noqa: E731
     serial = [eng.solve(p) for p in probs]        # warm-up (grows every buffer once)
     eng.batch_solve(probs)
@@ -208,7 +219,7 @@ def batched(local: int, flush, count: int = 256, reps: int = 3):
             "solves_per_s": count / best, "ms_per_batch": 1e3 * best,
             "serial_solves_per_s": count / ts, "serial_ms": 1e3 * ts,
             "speedup_vs_serial": ts / best, "identical_to_serial": same,
-            "unique_cs": sum(r.total_rows for r in serial), "reps": reps}
+            "unique_cs": sum(r.total_rows for r in serial), "reps": reps, "autotuned": tuned}
 
 
 def large_roofline(local: int, peak: float):
@@ -218,6 +229,7 @@ def large_roofline(local: int, peak: float):
     from vfb_b200 import synth
     p = vfb_b200.Problem.from_instance(synth.config_batch(count=3)[2])
     eng = vfb_b200.Engine(device=local, profile=True)
+    tuned = _tune_summary(eng.autotune([p], reps=2), "the instance")
     eng.solve(p)
     eng.solve(p)
     eng.profile_reset()
@@ -235,7 +247,7 @@ def large_roofline(local: int, peak: float):
     return {"instance": "mixed batch #2 (7 APs, 36 traces, size 9, 11.3M unique CS)",
             "kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "ms": ms, "launches": nl, "unique_cs": r.total_rows,
-            "kernels": per}
+            "kernels": per, "autotuned": tuned}
 
 
 def cpu_baseline(inst, budget_s: float):
@@ -283,6 +295,8 @@ def main():
     prob = vfb_b200.Problem.from_instance(inst)
     eng = vfb_b200.Engine(device=local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")   # > 126 MB L2
+    # k_p1 launch shape per level band, tuned on the workload before timing
+    table = eng.autotune([prob], reps=2)
 
     for _ in range(args.warmup):
         r = eng.solve(prob)
@@ -316,6 +330,7 @@ def main():
 
     # profiling pass: per-kernel CUDA-event times over the same solves
     peng = vfb_b200.Engine(device=local, profile=True)
+    peng.set_tune(table)
     for _ in range(args.warmup):
         peng.solve(prob)
     peng.profile_reset()
@@ -351,7 +366,8 @@ def main():
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "parallelism": f"replicas{world}",
-                   "l2": "flushed before every step (256 MB write)"},
+                   "l2": "flushed before every step (256 MB write)",
+                   "launch_shape": _tune_summary(table, "the workload (autotuned before the warm-up)")},
         "time_to_formula_ms": 1e3 * statistics.median(wall_s),
         "candidates_per_s": world * cands / dev_total,
         "time_to_formula_device_ms": 1e3 * statistics.median(dev_s),
