@@ -49,75 +49,107 @@ __device__ __forceinline__ void step_entry() {
 // tiling, buffer checks.  Records the plan (planned = k, plan_*) or asks the
 // host for memory (NEED_MEM, planned = 0).
 __device__ void plan_one(InstDev& I) {
-  const int k = I.level, c1 = atom_level(I);
-  const uint64_t* n = I.lcount;
-  I.lstart[k] = I.lstart[k - 1] + n[k - 1];
+  // Everything the plan reads is loaded first: the plan runs on one thread,
+  // and a load issued after a store to the record waits for that store.
+  const int k = I.level, weighted = I.weighted, on_the_fly = I.on_the_fly;
+  const int c1 = atom_level(I), Ln = not_level(I, k);
+  const int wA = op_cost(I, OP_AND), wO = op_cost(I, OP_OR), wX = op_cost(I, OP_X), wF = op_cost(I, OP_F),
+            wG = op_cost(I, OP_G), wU = op_cost(I, OP_U);
+  uint64_t n[kMaxSize + 1];
+  for (int i = 0; i <= k; ++i) n[i] = I.lcount[i];
+  const uint64_t lstart_prev = I.lstart[k - 1];
+  const uint64_t keys = I.keys, table_cap = I.table_mask + 1, bitmap_words = I.bitmap_words,
+                 row_cap = I.row_cap, tent_cap = I.tent_cap, promote_above = I.promote_above;
+  const int attempt = I.attempt, attempt_level = I.attempt_level;
+  const uint64_t lstart_k = lstart_prev + n[k - 1];
+  I.lstart[k] = lstart_k;
   // candidate blocks in canonical order: ~ & | X F G U; a unary operator of
   // cost c reads level k - c, & | over splits (i, k - c - i) with i <= k - c - i,
   // U over every split (LTL_BS.cu:1226-1488; unit costs: the size order)
   uint64_t g = 0;
-  const int Ln = not_level(I, k);
   I.base_not = g;
   if (Ln >= 0) g += n[Ln];
   for (int pass = 0; pass < 2; ++pass) {
-    const int w = op_cost(I, pass ? OP_OR : OP_AND);
+    const int w = pass ? wO : wA;
     for (int i = c1; 2 * i <= k - w; ++i) {
       const int j = k - w - i;
       (pass ? I.base_or : I.base_and)[i] = g;
       g += n[i] * n[j];
     }
   }
-  uint64_t* const ub[3] = {&I.base_x, &I.base_f, &I.base_g};
-  for (int o = 0; o < 3; ++o) {
-    const int L = k - op_cost(I, OP_X + o);
-    *ub[o] = g;
-    if (L >= c1) g += n[L];
-  }
   {
-    const int w = op_cost(I, OP_U);
-    for (int i = c1; k - w - i >= c1; ++i) {
-      I.base_u[i] = g;
-      g += n[i] * n[k - w - i];
+    const int ws[3] = {wX, wF, wG};
+    uint64_t bx[3];
+#pragma unroll
+    for (int o = 0; o < 3; ++o) {
+      const int L = k - ws[o];
+      bx[o] = g;
+      if (L >= c1) g += n[L];
     }
+    I.base_x = bx[0];
+    I.base_f = bx[1];
+    I.base_g = bx[2];
+  }
+  for (int i = c1; k - wU - i >= c1; ++i) {
+    I.base_u[i] = g;
+    g += n[i] * n[k - wU - i];
   }
   I.cands = g;
   // operand groups: the unary operators by operand level (bits ~ X F G), the
   // binary ones by level pair la <= lb (bits &, |, la U lb, lb U la); with
   // unit costs one unary group and one group per split, as the reference's
-  // launches fuse them
+  // launches fuse them.  The tiles of every staged height 2^0..2^5 are summed
+  // on the way.
   int ng = 0;
-  if (!I.weighted) {
+  uint64_t tl[6] = {0, 0, 0, 0, 0, 0};
+  auto add_tiles = [&](int kind, int la, int lb) {
+    if (kind == 0) {
+      const uint64_t st = (n[la] + kTS - 1) / kTS;
+#pragma unroll
+      for (int u = 0; u < 6; ++u) tl[u] += st;
+    } else {
+      const bool qleft = (la == lb) || (n[la] <= n[lb]);
+      const uint64_t nS = qleft ? n[lb] : n[la], nQ = qleft ? n[la] : n[lb];
+      const uint64_t st = (nS + kTS - 1) / kTS;
+#pragma unroll
+      for (int u = 0; u < 6; ++u) tl[u] += st * ((nQ + (1ULL << u) - 1) >> u);
+    }
+  };
+  if (!weighted) {
     // unit costs: one unary group over level k-1, one group per size split
     I.grp_kind[0] = 0; I.grp_la[0] = (uint8_t)(k - 1); I.grp_lb[0] = 0; I.grp_mask[0] = 0xF;
+    add_tiles(0, k - 1, 0);
     ng = 1;
     for (int i = 1; 2 * i <= k - 1; ++i, ++ng) {
       I.grp_kind[ng] = 1;
       I.grp_la[ng] = (uint8_t)i;
       I.grp_lb[ng] = (uint8_t)(k - 1 - i);
       I.grp_mask[ng] = (uint8_t)(i == k - 1 - i ? 7 : 15);
+      add_tiles(1, i, k - 1 - i);
     }
-  }
-  auto unary = [&](int L, int bit) {
-    if (L < c1) return;
-    for (int q = 0; q < ng; ++q)
-      if (I.grp_kind[q] == 0 && I.grp_la[q] == L) { I.grp_mask[q] |= (uint8_t)(1 << bit); return; }
-    if (ng >= kGroups) return;
-    I.grp_kind[ng] = 0; I.grp_la[ng] = (uint8_t)L; I.grp_lb[ng] = 0; I.grp_mask[ng] = (uint8_t)(1 << bit);
-    ++ng;
-  };
-  auto binary = [&](int la, int lb, int bits) {
-    for (int q = 0; q < ng; ++q)
-      if (I.grp_kind[q] == 1 && I.grp_la[q] == la && I.grp_lb[q] == lb) { I.grp_mask[q] |= (uint8_t)bits; return; }
-    if (ng >= kGroups) return;
-    I.grp_kind[ng] = 1; I.grp_la[ng] = (uint8_t)la; I.grp_lb[ng] = (uint8_t)lb; I.grp_mask[ng] = (uint8_t)bits;
-    ++ng;
-  };
-  if (I.weighted) unary(Ln, 0);
-  if (I.weighted) unary(k - op_cost(I, OP_X), 1);
-  if (I.weighted) unary(k - op_cost(I, OP_F), 2);
-  if (I.weighted) unary(k - op_cost(I, OP_G), 3);
-  if (I.weighted) {
-    const int s3 = k - op_cost(I, OP_AND), s4 = k - op_cost(I, OP_OR), s8 = k - op_cost(I, OP_U);
+  } else {
+    // weighted: a level (pair) may serve several operators, so the groups
+    // are collected first, then their tiles summed
+    auto unary = [&](int L, int bit) {
+      if (L < c1) return;
+      for (int q = 0; q < ng; ++q)
+        if (I.grp_kind[q] == 0 && I.grp_la[q] == L) { I.grp_mask[q] |= (uint8_t)(1 << bit); return; }
+      if (ng >= kGroups) return;
+      I.grp_kind[ng] = 0; I.grp_la[ng] = (uint8_t)L; I.grp_lb[ng] = 0; I.grp_mask[ng] = (uint8_t)(1 << bit);
+      ++ng;
+    };
+    auto binary = [&](int la, int lb, int bits) {
+      for (int q = 0; q < ng; ++q)
+        if (I.grp_kind[q] == 1 && I.grp_la[q] == la && I.grp_lb[q] == lb) { I.grp_mask[q] |= (uint8_t)bits; return; }
+      if (ng >= kGroups) return;
+      I.grp_kind[ng] = 1; I.grp_la[ng] = (uint8_t)la; I.grp_lb[ng] = (uint8_t)lb; I.grp_mask[ng] = (uint8_t)bits;
+      ++ng;
+    };
+    unary(Ln, 0);
+    unary(k - wX, 1);
+    unary(k - wF, 2);
+    unary(k - wG, 3);
+    const int s3 = k - wA, s4 = k - wO, s8 = k - wU;
     const int sums[3] = {s3, s4, s8};
     for (int q = 0; q < 3; ++q) {
       const int sm = sums[q];
@@ -132,54 +164,56 @@ __device__ void plan_one(InstDev& I) {
         binary(i, j, bits);
       }
     }
+    for (int q = 0; q < ng; ++q) add_tiles(I.grp_kind[q], I.grp_la[q], I.grp_lb[q]);
   }
   I.ngroups = ng;
-  // P1 tiling: kTS stream rows x tq staged rows per tile; small levels get
-  // shorter tiles so that they still spread over every SM
-  // (tq is a power of two: tile counts by shifts, not 64-bit divisions).
-  // The level's band of the tune table bounds the staged height, sets the
-  // tile count to reach and the CTAs to launch.
+  // P1 tiling: kTS stream rows x tq staged rows per tile.  The staged height
+  // is the largest power of two within the band's bound whose tile count
+  // reaches the band's target (small levels get shorter tiles so that they
+  // still spread over every SM and end in a short last wave), else 1.  The
+  // level's band of the tune table also sets the CTAs to launch.
   const int band = tune_band(g);
   const int rows_cap = I.tune_rows[band] ? (I.tune_rows[band] < kTQ ? I.tune_rows[band] : kTQ) : kTQDefault;
   const uint64_t target = I.tune_tiles[band] ? 1ULL << I.tune_tiles[band] : (uint64_t)kP1TileTarget;
   I.p1_blocks = I.tune_blocks[band];
-  uint64_t t = 0;
   int lg = 0;
-  while ((1 << (lg + 1)) <= rows_cap) ++lg;
-  for (;;) {
-    t = 0;
+  uint64_t t = tl[0];
+#pragma unroll
+  for (int u = 1; u < 6; ++u)
+    if ((1 << u) <= rows_cap && tl[u] >= target) { lg = u; t = tl[u]; }
+  I.tq = 1 << lg;
+  // group boundaries in tiles (ph_p1 reads the first ngroups of them)
+  {
+    uint64_t acc = 0;
     I.grp_prefix[0] = 0;
     for (int q = 0; q < ng; ++q) {
-      if (I.grp_kind[q] == 0) {
-        t += (n[I.grp_la[q]] + kTS - 1) / kTS;
+      const int kind = weighted ? I.grp_kind[q] : (q > 0);
+      const int la = weighted ? I.grp_la[q] : (q ? q : k - 1);
+      const int lb = weighted ? I.grp_lb[q] : (q ? k - 1 - q : 0);
+      if (kind == 0) {
+        acc += (n[la] + kTS - 1) / kTS;
       } else {
-        const int i = I.grp_la[q], j = I.grp_lb[q];
-        const bool qleft = (i == j) || (n[i] <= n[j]);
-        const uint64_t nS = qleft ? n[j] : n[i], nQ = qleft ? n[i] : n[j];
+        const bool qleft = (la == lb) || (n[la] <= n[lb]);
+        const uint64_t nS = qleft ? n[lb] : n[la], nQ = qleft ? n[la] : n[lb];
         const uint64_t qt = (nQ + (1ULL << lg) - 1) >> lg, st = (nS + kTS - 1) / kTS;
         I.grp_qtiles[q] = (uint32_t)qt;
-        t += st * qt;
+        acc += st * qt;
       }
-      I.grp_prefix[q + 1] = t;
+      I.grp_prefix[q + 1] = acc;
     }
-    if (t >= target || lg == 0) break;
-    --lg;
   }
-  I.tq = 1 << lg;
-  for (int q = ng; q < kGroups; ++q) I.grp_prefix[q + 1] = t;
-  const uint64_t words = I.on_the_fly ? 0 : (g + 31) / 32;
-  const uint64_t cap = I.table_mask + 1;
+  const uint64_t words = on_the_fly ? 0 : (g + 31) / 32;
   // new keys of this level: at most all candidates; expect ~8x growth
   const uint64_t grow = 8 * n[k - 1] + 4096;
   const uint64_t est = g < grow ? g : grow;
   int need = 0;
   if (g >= (1ULL << kPayShift)) need |= NEED_LIMIT;
-  if (!I.on_the_fly) {   // an on-the-fly level stores nothing
-    if (g > I.promote_above) need |= NEED_PROMOTE;
-    if (words > I.bitmap_words) { need |= NEED_BITMAP; I.need_amount[0] = words; }
-    if (2 * (I.keys + est) > cap) { need |= NEED_TABLE; I.need_amount[1] = 4 * (I.keys + est); }
-    if (I.lstart[k] + est > I.row_cap) { need |= NEED_ROWS; I.need_amount[3] = I.lstart[k] + est; }
-    if (est > I.tent_cap) { need |= NEED_LIST; I.need_amount[2] = est; }
+  if (!on_the_fly) {   // an on-the-fly level stores nothing
+    if (g > promote_above) need |= NEED_PROMOTE;
+    if (words > bitmap_words) { need |= NEED_BITMAP; I.need_amount[0] = words; }
+    if (2 * (keys + est) > table_cap) { need |= NEED_TABLE; I.need_amount[1] = 4 * (keys + est); }
+    if (lstart_k + est > row_cap) { need |= NEED_ROWS; I.need_amount[3] = lstart_k + est; }
+    if (est > tent_cap) { need |= NEED_LIST; I.need_amount[2] = est; }
   }
   if (need) {
     I.status = ST_NEED_MEM;
@@ -188,7 +222,7 @@ __device__ void plan_one(InstDev& I) {
   } else {
     I.plan_tiles = t;
     I.plan_words = words;
-    I.plan_tchunks = I.on_the_fly ? 0 : (cap + kScanSlots - 1) / kScanSlots;
+    I.plan_tchunks = on_the_fly ? 0 : (table_cap + kScanSlots - 1) / kScanSlots;
     I.planned = k;
     I.p1_done = 0;
     I.p1_step = t;
@@ -196,7 +230,7 @@ __device__ void plan_one(InstDev& I) {
     I.n_new = I.n_wins = I.probe_fail = I.n_newlist = 0;
     I.best_cand = I.best_sol = ~0ULL;
     I.sol_known = 0;
-    I.attempt = (I.attempt_level == k) ? I.attempt + 1 : 1;
+    I.attempt = (attempt_level == k) ? attempt + 1 : 1;
     I.attempt_level = k;
   }
 }
@@ -233,7 +267,7 @@ __device__ void ph_plan_prefix(const BatchDev& B) {
   for (int i = 0; i < kTickets; ++i) B.tickets[i] = 0;
 }
 
-__global__ void k_plan(BatchDev* Bp) {
+__global__ void __launch_bounds__(1024) k_plan(BatchDev* Bp) {
   const BatchDev B = *Bp;
   ph_plan(B, 0, 1);
   __syncthreads();
@@ -263,8 +297,12 @@ __device__ void ph_p1(const BatchDev& B) {
         // lane l holds group boundaries 2l+1 and 2l+2; the group is the number
         // of boundaries at or below the tile
         const int e1 = 2 * lane + 1, e2 = 2 * lane + 2;
-        const uint64_t gp1 = e1 < kGroups ? __ldcg(&Ip->grp_prefix[e1]) : ~0ULL;
-        const uint64_t gp2 = e2 < kGroups ? __ldcg(&Ip->grp_prefix[e2]) : ~0ULL;
+        // (boundaries past the level's groups are stale: read as never reached)
+        const int ngr = __ldcg(&Ip->ngroups);
+        uint64_t gp1 = e1 < kGroups ? __ldcg(&Ip->grp_prefix[e1]) : ~0ULL;
+        uint64_t gp2 = e2 < kGroups ? __ldcg(&Ip->grp_prefix[e2]) : ~0ULL;
+        if (e1 >= ngr) gp1 = ~0ULL;
+        if (e2 >= ngr) gp2 = ~0ULL;
         const int grp = __popc(__ballot_sync(0xffffffffu, gp1 <= local)) +
                         __popc(__ballot_sync(0xffffffffu, gp2 <= local));
         const int src = grp >= 1 ? (grp - 1) >> 1 : 0;
@@ -752,17 +790,23 @@ __device__ void finish_one(InstDev& I) {
     }
     return;
   }
-  I.built_cands = I.cands;
-  I.built_wins = I.n_wins;
-  I.built_scanned = (I.attempt == 1 && I.n_newlist <= I.tent_cap) ? I.n_newlist : I.table_mask + 1;
-  I.built_sol_known = I.sol_known;
-  I.keys += I.n_wins;
-  if (I.best_sol != ~0ULL) {
-    const uint64_t g = I.best_sol;
-    uint64_t lo = 0, hi = I.n_wins;   // first index with wins[idx] >= g
+  // the level's figures are read before the record is written (one thread:
+  // a load after a store to the record waits for the store)
+  const uint64_t cands = I.cands, wins = I.n_wins, newlist = I.n_newlist, tent = I.tent_cap,
+                 cap = I.table_mask + 1, best = I.best_sol, keys = I.keys;
+  const uint64_t* wlist = I.wins;
+  const int attempt = I.attempt, sol_known = I.sol_known, max_size = I.max_size;
+  I.built_cands = cands;
+  I.built_wins = wins;
+  I.built_scanned = (attempt == 1 && newlist <= tent) ? newlist : cap;
+  I.built_sol_known = sol_known;
+  I.keys = keys + wins;
+  if (best != ~0ULL) {
+    const uint64_t g = best;
+    uint64_t lo = 0, hi = wins;   // first index with wins[idx] >= g
     while (lo < hi) {
       const uint64_t mid = (lo + hi) >> 1;
-      if (I.wins[mid] < g) lo = mid + 1; else hi = mid;
+      if (wlist[mid] < g) lo = mid + 1; else hi = mid;
     }
     I.lcount[k] = lo + 1;
     I.lcands[k] = g + 1;
@@ -771,10 +815,10 @@ __device__ void finish_one(InstDev& I) {
     I.status = ST_FOUND;
     reconstruct(I, k, g);
   } else {
-    I.lcount[k] = I.n_wins;
-    I.lcands[k] = I.cands;
+    I.lcount[k] = wins;
+    I.lcands[k] = cands;
     I.res_size = k;
-    if (k >= I.max_size) I.status = ST_NOT_FOUND;
+    if (k >= max_size) I.status = ST_NOT_FOUND;
     else I.level = k + 1;
   }
 }
@@ -802,7 +846,7 @@ __global__ void __launch_bounds__(1024) k_advance(BatchDev* Bp, cudaGraphConditi
                                                   int loop, unsigned int max_iter) {
   __shared__ int s_run, s_need;
   __shared__ unsigned s_blocks;
-  __shared__ unsigned long long s_w[32];
+  __shared__ unsigned long long s_w3[32][3];
   __shared__ unsigned long long s_carry[3];
   step_entry();
   const BatchDev B = *Bp;
@@ -848,19 +892,20 @@ __global__ void __launch_bounds__(1024) k_advance(BatchDev* Bp, cudaGraphConditi
       B.status_out[b] = make_int2(I.status, I.need);
     }
     // inclusive prefixes over this block of instances, carried across blocks
-    unsigned long long tot;
-    const unsigned long long e0 = block_excl_scan(tiles, s_w, tot);
-    if (b < B.ninst) B.p1_prefix[b + 1] = s_carry[0] + e0 + tiles;
+    const unsigned long long v[3] = {tiles, chunks, tchunks};
+    unsigned long long ex[3], tot[3];
+    block_excl_scan3(v, s_w3, ex, tot);
+    if (b < B.ninst) {
+      B.p1_prefix[b + 1] = s_carry[0] + ex[0] + tiles;
+      B.chunk_prefix[b + 1] = s_carry[1] + ex[1] + chunks;
+      B.tscan_prefix[b + 1] = s_carry[2] + ex[2] + tchunks;
+    }
     __syncthreads();
-    if (threadIdx.x == 0) s_carry[0] += tot;
-    const unsigned long long e1 = block_excl_scan(chunks, s_w, tot);
-    if (b < B.ninst) B.chunk_prefix[b + 1] = s_carry[1] + e1 + chunks;
-    __syncthreads();
-    if (threadIdx.x == 0) s_carry[1] += tot;
-    const unsigned long long e2 = block_excl_scan(tchunks, s_w, tot);
-    if (b < B.ninst) B.tscan_prefix[b + 1] = s_carry[2] + e2 + tchunks;
-    __syncthreads();
-    if (threadIdx.x == 0) s_carry[2] += tot;
+    if (threadIdx.x == 0) {
+      s_carry[0] += tot[0];
+      s_carry[1] += tot[1];
+      s_carry[2] += tot[2];
+    }
     __syncthreads();
   }
   if (run) atomicOr(&s_run, 1);

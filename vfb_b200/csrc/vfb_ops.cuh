@@ -112,6 +112,46 @@ __device__ inline unsigned long long block_excl_scan(unsigned long long v, unsig
   return before + x - v;
 }
 
+// Three exclusive block scans at once (one pass of barriers): v[c] -> the
+// sum of v[c] over the threads before this one; total[c] = the block's sum.
+__device__ inline void block_excl_scan3(const unsigned long long (&v)[3], unsigned long long (*s_warp)[3],
+                                        unsigned long long (&excl)[3], unsigned long long (&total)[3]) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  unsigned long long x[3] = {v[0], v[1], v[2]};
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const unsigned long long y = __shfl_up_sync(0xffffffffu, x[c], o);
+      if (lane >= o) x[c] += y;
+    }
+  }
+  if (lane == 31) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) s_warp[wid][c] = x[c];
+  }
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      unsigned long long w = lane < nw ? s_warp[lane][c] : 0ULL;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+      }
+      if (lane < nw) s_warp[lane][c] = w;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    total[c] = s_warp[nw - 1][c];
+    excl[c] = (wid > 0 ? s_warp[wid - 1][c] : 0ULL) + x[c] - v[c];
+  }
+  __syncthreads();
+}
+
 __device__ __forceinline__ uint64_t apply_w(int op, uint64_t l, uint64_t r, int L) {
   switch (op) {
     case OP_NOT: return ~l & len_mask(L);
