@@ -19,6 +19,10 @@ cpu_baseline  the CPU restatement (single thread) on a bounded sample.
 --impl reference  the CPU restatement with OpenMP on every host core, same
         workload and metric (the reference itself is CUDA-only).
 
+--no-tune  keep the built-in k_p1 launch shape instead of autotuning it on
+        each workload first (for launch-list captures: the tuner's own solves
+        are many thousands of launches).
+
 N > 1 (torchrun): replicas -- every rank solves its own copy on its GPU; value
 is the units of all ranks over the slowest rank's time.
 """
@@ -175,6 +179,13 @@ def run_reference(args, inst):
     print(json.dumps(line), flush=True)
 
 
+def _tune(eng, probs, sample: str, enabled: bool):
+    """Autotune eng's launch shape on probs (when enabled); the summary for the line."""
+    if not enabled:
+        return {"sample": None, "bands": "built-in shape (--no-tune)"}
+    return _tune_summary(eng.autotune(probs, reps=2), sample)
+
+
 def _tune_summary(table: dict, sample: str) -> dict:
     """The autotuned k_p1 shape of the bands the sample's levels fell in:
     band -> [staged rows, log2 tile target, CTAs] (0: built-in), and the
@@ -185,7 +196,7 @@ def _tune_summary(table: dict, sample: str) -> dict:
             "p1_ms_tuned": round(sum(table["ms"]), 4), "p1_ms_builtin": round(sum(table["ms_default"]), 4)}
 
 
-def batched(local: int, flush, count: int = 256, reps: int = 3):
+def batched(local: int, flush, count: int = 256, reps: int = 3, tune: bool = True):
     """The mixed batch (seed 3): one vfb_batch_solve of every instance against
     one vfb_solve per instance on the same engine, both warm (device timeline
     of every call summed over the run, torch synchronised around it)."""
@@ -194,7 +205,7 @@ def batched(local: int, flush, count: int = 256, reps: int = 3):
     from vfb_b200 import synth
     probs = [vfb_b200.Problem.from_instance(i) for i in synth.config_batch(count=count)]
     eng = vfb_b200.Engine(device=local)
-    tuned = _tune_summary(eng.autotune(probs[:16], reps=2), "the batch's first 16 instances, solved one by one")
+    tuned = _tune(eng, probs[:16], "the batch's first 16 instances, solved one by one", tune)
     key = lambda r: (r.status, r.size, r.rpn, r.level_rows, r.level_cands)  # noqa: E731
     serial = [eng.solve(p) for p in probs]        # warm-up (grows every buffer once)
     eng.batch_solve(probs)
@@ -222,14 +233,14 @@ def batched(local: int, flush, count: int = 256, reps: int = 3):
             "unique_cs": sum(r.total_rows for r in serial), "reps": reps, "autotuned": tuned}
 
 
-def large_roofline(local: int, peak: float):
+def large_roofline(local: int, peak: float, tune: bool = True):
     """Per-kernel profile of the largest instance of the mixed batch (#2,
     11.3M unique CS): the kernels' rates on levels that fill the GPU."""
     import vfb_b200
     from vfb_b200 import synth
     p = vfb_b200.Problem.from_instance(synth.config_batch(count=3)[2])
     eng = vfb_b200.Engine(device=local, profile=True)
-    tuned = _tune_summary(eng.autotune([p], reps=2), "the instance")
+    tuned = _tune(eng, [p], "the instance", tune)
     eng.solve(p)
     eng.solve(p)
     eng.profile_reset()
@@ -271,6 +282,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="vfb", choices=["vfb", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=10.0)
+    ap.add_argument("--no-tune", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = _dist()
@@ -296,7 +308,7 @@ def main():
     eng = vfb_b200.Engine(device=local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")   # > 126 MB L2
     # k_p1 launch shape per level band, tuned on the workload before timing
-    table = eng.autotune([prob], reps=2)
+    table = eng.autotune([prob], reps=2) if not args.no_tune else None
 
     for _ in range(args.warmup):
         r = eng.solve(prob)
@@ -330,7 +342,7 @@ def main():
 
     # profiling pass: per-kernel CUDA-event times over the same solves
     peng = vfb_b200.Engine(device=local, profile=True)
-    peng.set_tune(table)
+    peng.set_tune(table)   # None: built-in
     for _ in range(args.warmup):
         peng.solve(prob)
     peng.profile_reset()
@@ -367,7 +379,8 @@ def main():
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "parallelism": f"replicas{world}",
                    "l2": "flushed before every step (256 MB write)",
-                   "launch_shape": _tune_summary(table, "the workload (autotuned before the warm-up)")},
+                   "launch_shape": _tune_summary(table, "the workload (autotuned before the warm-up)")
+                   if table else {"sample": None, "bands": "built-in shape (--no-tune)"}},
         "time_to_formula_ms": 1e3 * statistics.median(wall_s),
         "candidates_per_s": world * cands / dev_total,
         "time_to_formula_device_ms": 1e3 * statistics.median(dev_s),
@@ -379,8 +392,8 @@ def main():
         "kernels": [{"name": p[0], "launches": p[1], "ms": p[2], "bytes": p[3]} for p in prof],
         "clocks": clk.summary(),
     }
-    line["batched"] = batched(local, flush)
-    line["large_instance"] = large_roofline(local, peak)
+    line["batched"] = batched(local, flush, tune=not args.no_tune)
+    line["large_instance"] = large_roofline(local, peak, tune=not args.no_tune)
     line["cpu_baseline"] = cpu_baseline(inst, args.cpu_budget)
     print(json.dumps(line), flush=True)
     if world > 1:
