@@ -86,3 +86,31 @@ def test_sliced_levels_equal_solo(engine):
         engine.serve_limits(0.8, 0)
     for (t, prob), got in zip(stream, results):
         assert _key(got) == _key(engine.solve(prob))
+
+
+def test_oversubscribed_memory_waits_instead_of_failing():
+    # four requests admitted together whose buffers do not all fit the
+    # budget at once: a growth that finds the memory held by the others waits
+    # (or its request restarts later) instead of failing, so every result is
+    # still the solo one
+    probs = []
+    for seed in (4242, 4243, 4244, 4245):
+        inst = cases.random_instance(seed, 4, 5, 5, 16, 8)
+        inst.neg[0] = inst.pos[0]          # unsatisfiable: every level up to size 8 is built
+        probs.append(vfb_b200.Problem.from_instance(inst))
+    with vfb_b200.Engine() as eng:
+        full = [eng.solve(p) for p in probs]
+    assert all(r.status == vfb_b200.NOT_FOUND for r in full)
+    budget = None   # the smallest of these budgets that holds each request alone
+    for mb in (32, 48, 64, 96, 128, 192, 256):
+        with vfb_b200.Engine(mem_limit_bytes=mb << 20) as eng:
+            if all(_key(eng.solve(p)) == _key(f) for p, f in zip(probs, full)):
+                budget = mb << 20
+                break
+    assert budget is not None
+    with vfb_b200.Engine(mem_limit_bytes=budget) as eng:
+        # admit all four at once; no per-request cap below the device budget
+        eng.serve_limits(1.0, 4 * budget)
+        results, _, _ = serve.run_stream(eng, [(0.0, p) for p in probs], slots=4, max_steps=20000)
+    for got, want in zip(results, full):
+        assert _key(got) == _key(want)

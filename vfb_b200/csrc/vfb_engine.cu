@@ -738,6 +738,7 @@ struct Engine {
       d.rows = (uint64_t*)pr;
       d.origin = (uint64_t*)po;
       d.row_cap = std::min<uint64_t>(g1 / ((size_t)d.TP * 8), g2 / 8);
+      d.need &= ~NEED_ROWS;   // a later part that fails leaves this one done
     }
     if (need & NEED_TABLE) {
       const uint64_t cap = d.table_mask + 1;
@@ -757,6 +758,7 @@ struct Engine {
       dfree(d.table);
       d.table = (Slot*)pt;
       d.table_mask = slots - 1;
+      d.need &= ~NEED_TABLE;
     }
     if (need & NEED_BITMAP) {
       const uint64_t want = std::max<uint64_t>(2 * d.bitmap_words, d.need_amount[0] + d.need_amount[0] / 4);
@@ -766,6 +768,7 @@ struct Engine {
       dfree(d.bitmap);
       d.bitmap = (uint32_t*)pb;
       d.bitmap_words = g1 / 4;
+      d.need &= ~NEED_BITMAP;
     }
     if (need & NEED_LIST) {
       const uint64_t want = std::max<uint64_t>(2 * d.tent_cap, d.need_amount[2] + d.need_amount[2] / 4);
@@ -774,6 +777,7 @@ struct Engine {
       dfree(d.wins);
       d.wins = (uint64_t*)pw;
       d.tent_cap = g1 / 8;
+      d.need &= ~NEED_LIST;
     }
     d.status = ST_RUNNING;
     d.need = 0;
@@ -1200,6 +1204,8 @@ struct Engine {
     std::vector<char> busy;
     std::deque<Pending> queue;
     std::vector<uint64_t> proj;   // projected bytes of each busy slot after its next level
+    std::vector<Pending> req;     // the request each busy slot holds (requeued if it is evicted)
+    uint64_t evictions = 0;       // requests evicted and queued again (memory held by the others)
     InstDev* h_inst = nullptr;    // pinned mirror of the slot records
     int p1_smem = 0;
     double budget_frac = 0.8;     // admission: projected bytes of all slots <= budget_frac * budget
@@ -1232,6 +1238,8 @@ struct Engine {
     sv.tag.assign(slots, 0);
     sv.busy.assign(slots, 0);
     sv.proj.assign(slots, 0);
+    sv.req.clear();
+    sv.req.resize(slots);
     sv.budget_frac = sv_budget_frac;
     sv.request_bytes = sv_request_bytes ? sv_request_bytes : (uint64_t)(mem_limit / 4);
     sv.step_cands = sv_step_cands;
@@ -1344,6 +1352,11 @@ struct Engine {
           if (hb <= sv.request_bytes) c = h;
         }
         s = alloc_buffers(H, c.rows, c.slots, c.words, c.tents);
+        if (s == VFB_OOM && nbusy > 0) {
+          // the memory is held by the requests on the device: admit later
+          H = InstHost{};
+          break;
+        }
         H.d.promote_above = ~0ULL;
         H.d.p1_quota = sv.step_cands;
       }
@@ -1375,6 +1388,9 @@ struct Engine {
       sv.proj[i] = inst_bytes(H.d);
       committed += sv.proj[i];
       ++nbusy;
+      sv.req[i] = std::move(sv.queue.front());
+      sv.req[i].in.words = sv.req[i].words.data();
+      sv.req[i].in.lengths = sv.req[i].lengths.data();
       sv.queue.pop_front();
       admitted = true;
     }
@@ -1398,21 +1414,67 @@ struct Engine {
       if (e != cudaSuccess) { last_error = e; return dev_fail(__LINE__); }
       ++c_launch;
     }
-    // 3. growth and 4. harvest
-    std::vector<int> fin;
+    // 3. growth and 4. harvest.  A growth that finds the device memory held
+    // by other requests waits: the record (with whatever part did grow) goes
+    // back to the device still asking, and the growth is tried again after
+    // the next step.  When no request can go on (every busy one waits and
+    // none finished), the waiting request with the fewest levels built is
+    // evicted and queued again at the front, to restart once memory frees;
+    // a request that waits alone cannot grow at all and goes on as a solo
+    // solve would, its level tested on the fly.  Results stay those of solo
+    // solves.
+    std::vector<int> fin, waiting;
+    bool progress = false;
     for (int i = 0; i < sv.cap; ++i) {
       if (!sv.busy[i]) continue;
       const int st = h_status[i].x;
       if (st == ST_NEED_MEM) {
         const vfb_status g = grow(sv.H[i], i, sv.request_bytes);
-        if (g != VFB_OK) {
+        if (g == VFB_OOM) {
+          InstDev& d = sv.H[i].d;
+          d.status = ST_NEED_MEM;
+          if (cudaMemcpyAsync(dInst + i, &d, sizeof(InstDev), cudaMemcpyHostToDevice, stream) != cudaSuccess)
+            return dev_fail(__LINE__);
+          c_h2d += sizeof(InstDev);
+          waiting.push_back(i);
+        } else if (g != VFB_OK) {
           sv.H[i].fail = g;
           const int err = ST_ERROR;
           cudaMemcpyAsync(&dInst[i].status, &err, sizeof(int), cudaMemcpyHostToDevice, stream);
           fin.push_back(i);
+        } else {
+          progress = true;
         }
       } else if (st == ST_FOUND || st == ST_NOT_FOUND || st == ST_ERROR || st == ST_LIMIT) {
         fin.push_back(i);
+      } else if (st == ST_RUNNING) {
+        progress = true;
+      }
+    }
+    if (!progress && fin.empty() && !waiting.empty()) {
+      if (waiting.size() == 1) {
+        const int i = waiting[0];
+        InstDev& d = sv.H[i].d;
+        d.on_the_fly = 1;
+        d.status = ST_RUNNING;
+        d.need = 0;
+        d.planned = 0;
+        if (cudaMemcpyAsync(dInst + i, &d, sizeof(InstDev), cudaMemcpyHostToDevice, stream) != cudaSuccess)
+          return dev_fail(__LINE__);
+        c_h2d += sizeof(InstDev);
+      } else {
+        int v = waiting[0];
+        for (int i : waiting)
+          if (sv.H[i].d.level <= sv.H[v].d.level) v = i;
+        free_buffers(sv.H[v]);
+        sv.H[v] = InstHost{};
+        sv.busy[v] = 0;
+        sv.queue.push_front(std::move(sv.req[v]));
+        sv.queue.front().in.words = sv.queue.front().words.data();
+        sv.queue.front().in.lengths = sv.queue.front().lengths.data();
+        const int idle = ST_IDLE;
+        cudaMemcpyAsync(&dInst[v].status, &idle, sizeof(int), cudaMemcpyHostToDevice, stream);
+        ++sv.evictions;
       }
     }
     for (int i : fin) {

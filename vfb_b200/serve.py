@@ -34,15 +34,19 @@ def percentile(xs, q):
     return xs[i]
 
 
-def run_stream(engine: Engine, stream, slots: int = 256, max_traces: int = 64):
-    """Returns (results by index, latencies by index, makespan seconds)."""
+def run_stream(engine: Engine, stream, slots: int = 256, max_traces: int = 64, max_steps: int = 0):
+    """Returns (results by index, latencies by index, makespan seconds).
+    max_steps > 0: raise RuntimeError after that many serve steps."""
     engine.serve_open(slots, max_traces)
     n = len(stream)
     results, finish = [None] * n, [0.0] * n
-    nxt, done = 0, 0
+    nxt, done, steps = 0, 0, 0
     t0 = time.perf_counter()
     try:
         while done < n:
+            steps += 1
+            if max_steps and steps > max_steps:
+                raise RuntimeError(f"stream not served within {max_steps} steps ({done}/{n} done)")
             now = time.perf_counter() - t0
             while nxt < n and stream[nxt][0] <= now:
                 engine.serve_submit(stream[nxt][1], nxt)
@@ -70,7 +74,10 @@ def request_stream(seed: int = 4, count: int = 2000, rate: float = 100.0, large_
             for t, inst in synth.config_serving(seed, count, rate, large_frac)]
 
 
-def summarize(rate, res, lat, span, slots):
+def summarize(rate, res, lat, span, slots, large=None):
+    """Status counts, latency percentiles and throughput of one served stream;
+    with large (a flag per request), the percentiles of the large-shape and
+    the other requests apart as well."""
     by = {}
     for r in res:
         name = "missing" if r is None else {0: "found", 1: "not_found", 2: "limit", 3: "oom"}.get(
@@ -79,7 +86,18 @@ def summarize(rate, res, lat, span, slots):
     return {"rate_req_per_s": rate, "requests": len(res), "status": by,
             "p50_ms": 1e3 * percentile(lat, 50), "p95_ms": 1e3 * percentile(lat, 95),
             "p99_ms": 1e3 * percentile(lat, 99), "mean_ms": 1e3 * statistics.mean(lat),
-            "solves_per_s": len(res) / span, "makespan_s": span, "slots": slots}
+            "solves_per_s": len(res) / span, "makespan_s": span, "slots": slots,
+            **({} if large is None else _by_class(lat, large))}
+
+
+def _by_class(lat, large):
+    out = {}
+    for name, want in (("mixed", False), ("large", True)):
+        sub = [x for x, f in zip(lat, large) if f == want]
+        if sub:
+            out[name] = {"requests": len(sub), "p50_ms": 1e3 * percentile(sub, 50),
+                         "p95_ms": 1e3 * percentile(sub, 95), "p99_ms": 1e3 * percentile(sub, 99)}
+    return out
 
 
 def main():
@@ -101,11 +119,13 @@ def main():
     eng.serve_limits(0.8, int(args.request_gb * (1 << 30)), args.step_cands)
     for rate in rates:
         count = args.count if not args.rates else min(args.count, max(50, int(args.window * rate)))
-        stream = request_stream(args.seed, count, rate, args.large_frac)
+        insts = synth.config_serving(args.seed, count, rate, args.large_frac)
+        stream = [(t, Problem.from_instance(inst)) for t, inst in insts]
+        large = [inst.name == "large" for _, inst in insts]
         # warm the kernels (module load, graph capture) outside the measured stream
         run_stream(eng, [(0.0, p) for _, p in stream[:4] if p.num_traces < 63] or stream[:1], args.slots)
         res, lat, span = run_stream(eng, stream, args.slots)
-        print(json.dumps(summarize(rate, res, lat, span, args.slots)), flush=True)
+        print(json.dumps(summarize(rate, res, lat, span, args.slots, large)), flush=True)
     eng.close()
 
 
