@@ -278,7 +278,7 @@ def cpu_baseline(inst, budget_s: float):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="vfb", choices=["vfb", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=10.0)
