@@ -15,6 +15,7 @@ importing the engine on a machine without the built library or a B200 raises.
 """
 from __future__ import annotations
 
+import array
 import ctypes
 import os
 from dataclasses import dataclass, field
@@ -43,6 +44,10 @@ class _Instance(ctypes.Structure):
                 ("num_pos", ctypes.c_int), ("words", ctypes.POINTER(ctypes.c_uint64)),
                 ("lengths", ctypes.POINTER(ctypes.c_int)), ("max_size", ctypes.c_int),
                 ("rlx_type", ctypes.c_int)]
+
+
+_P_U64 = ctypes.POINTER(ctypes.c_uint64)
+_P_INT = ctypes.POINTER(ctypes.c_int)
 
 
 class _Result(ctypes.Structure):
@@ -187,11 +192,13 @@ class Problem:
                    inst.max_size, inst.rlx_type, max(l for l, _ in traces))
 
     def _cstruct(self):
-        w = (ctypes.c_uint64 * max(1, len(self.words)))(*self.words)
-        ln = (ctypes.c_int * max(1, len(self.lengths)))(*self.lengths)
+        # the C arrays are Python array buffers (one C-level conversion each);
+        # the caller keeps them alive until the call returns
+        w = array.array("Q", self.words or [0])
+        ln = array.array("i", self.lengths or [0])
         s = _Instance(self.num_vars, self.num_traces, self.num_pos,
-                      ctypes.cast(w, ctypes.POINTER(ctypes.c_uint64)),
-                      ctypes.cast(ln, ctypes.POINTER(ctypes.c_int)), self.max_size, self.rlx_type)
+                      ctypes.cast(w.buffer_info()[0], _P_U64), ctypes.cast(ln.buffer_info()[0], _P_INT),
+                      self.max_size, self.rlx_type)
         return s, (w, ln)
 
 
@@ -230,9 +237,9 @@ class Result:
 
 def _result(r: _Result) -> Result:
     k = max(0, min(r.size, MAX_SIZE))
-    rpn = [r.rpn[i] if r.rpn[i] >= 0 else OPS[-r.rpn[i] - 1] for i in range(r.rpn_len)]
-    return Result(r.status, r.size, rpn, [r.level_rows[i] for i in range(1, k + 1)],
-                  [r.level_cands[i] for i in range(1, k + 1)], r.total_rows, r.solution_index,
+    rpn = [x if x >= 0 else OPS[-x - 1] for x in r.rpn[:max(0, min(r.rpn_len, MAX_SIZE))]]
+    return Result(r.status, r.size, rpn, r.level_rows[1:k + 1],
+                  r.level_cands[1:k + 1], r.total_rows, r.solution_index,
                   r.seconds, r.device_seconds, r.h2d_bytes, r.d2h_bytes, r.kernel_launches)
 
 

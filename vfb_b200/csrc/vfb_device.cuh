@@ -25,6 +25,9 @@ constexpr int kP1TileTarget = 4096;   // shrink the staged height until a level 
 // of 4^b to 4^(b+1)-1 candidates, the last band every larger level
 constexpr int kTuneBands = 16;
 constexpr int kMaxProbes = 4096;      // bounded linear probing
+// first buffers of at most this many table + bitmap bytes are initialised by
+// k_init's CTA for the instance instead of by two memsets each
+constexpr uint64_t kInitFillMax = 4ull << 20;
 constexpr uint64_t kEmpty = ~0ULL;
 constexpr int kPayShift = 58;         // payload = level << 58 | candidate index
 constexpr uint64_t kIdxMask = (1ULL << kPayShift) - 1;
@@ -119,7 +122,8 @@ struct InstDev {
   unsigned long long n_new, n_wins, probe_fail;
   unsigned long long best_cand;  // min candidate index whose CS satisfies the sample (P1)
   unsigned long long best_sol;   // min candidate index of a solution owning its key
-  int sol_known, pad2;           // best_sol settled before the rows were emitted
+  int sol_known;                 // best_sol settled before the rows were emitted
+  int fill;                      // 1: the table and the bitmap are still to be initialised (k_init)
   unsigned long long n_newlist;  // slots of keys first inserted by this level's P1 (listed in wins)
   int attempt, attempt_level;    // attempts at the current level (> 1: a retry after growth)
   int planned, p1_tail;          // level the current plan (bases, tiling) was made for (0: none);

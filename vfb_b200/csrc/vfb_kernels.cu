@@ -1252,6 +1252,13 @@ __global__ void k_init(BatchDev* Bp) {
   for (int b = blockIdx.x; b < B.ninst; b += gridDim.x) {
     InstDev& I = B.inst[b];
     if (I.status != ST_RUNNING || I.level != 1) continue;
+    if (I.fill) {
+      // empty table (every word ~0) and clear owner bitmap
+      ulonglong2* tab = reinterpret_cast<ulonglong2*>(I.table);
+      const uint64_t nt = (I.table_mask + 1) * (sizeof(Slot) / sizeof(ulonglong2));
+      for (uint64_t x = threadIdx.x; x < nt; x += blockDim.x) tab[x] = make_ulonglong2(~0ULL, ~0ULL);
+      for (uint64_t x = threadIdx.x; x < I.bitmap_words; x += blockDim.x) I.bitmap[x] = 0u;
+    }
     if (threadIdx.x == 0) { s_first = ~0ULL; s_new = 0; }
     __syncthreads();
     for (int v = threadIdx.x; v < I.A; v += blockDim.x) {
@@ -1271,6 +1278,7 @@ __global__ void k_init(BatchDev* Bp) {
     }
     __syncthreads();
     if (threadIdx.x == 0) {
+      I.fill = 0;
       // the propositions are the level of their cost c1 (1 with unit costs);
       // the levels below it are empty
       const int c1 = atom_level(I);
