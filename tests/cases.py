@@ -56,3 +56,26 @@ def planted_cases(count: int = 6, max_size_extra: int = 2):
                                       size + max_size_extra, name=f"planted{s}")
         out.append(inst)
     return out
+
+
+def unsatisfiable_cases(seeds=(4242, 4243, 4244, 4245)):
+    """Instances with a positive trace equal to a negative one: nothing solves
+    them, so every level up to max size 8 is built (about 200k rows each)."""
+    out = []
+    for seed in seeds:
+        inst = random_instance(seed, 4, 5, 5, 16, 8)
+        inst.neg[0] = inst.pos[0]
+        out.append(inst)
+    return out
+
+
+def smallest_solo_budget(probs, want, sizes_mb=(32, 48, 64, 96, 128, 192, 256)):
+    """The smallest device budget (bytes) under which every problem, solved
+    alone in a fresh context, returns the result in want (GPU only)."""
+    import vfb_b200
+    key = lambda r: (r.status, r.size, r.rpn, r.level_rows, r.level_cands)  # noqa: E731
+    for mb in sizes_mb:
+        with vfb_b200.Engine(mem_limit_bytes=mb << 20) as eng:
+            if all(key(eng.solve(p)) == key(w) for p, w in zip(probs, want)):
+                return mb << 20
+    return None

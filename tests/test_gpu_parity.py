@@ -169,3 +169,37 @@ def test_on_the_fly_level(engine):
         else:
             assert r.status == vfb_b200.OOM
     assert hits >= 1
+
+
+def test_second_context_gets_the_memory_the_first_released():
+    # a context that solved many instances one by one keeps only its last
+    # working set cached (not every superseded buffer size); a second context
+    # created afterwards in the same process has the memory for the whole
+    # batch and returns the same results
+    probs = [vfb_b200.Problem.from_instance(i) for i in synth.config_batch(count=256)]
+    key = lambda r: (r.status, r.size, r.rpn, r.level_rows, r.level_cands, r.solution_index)  # noqa: E731
+    with vfb_b200.Engine() as first:
+        want = [first.solve(p) for p in probs]
+        with vfb_b200.Engine() as second:
+            got = second.batch_solve(probs)
+    assert [key(r) for r in got] == [key(r) for r in want]
+
+
+def test_batch_under_memory_pressure_equals_solo():
+    # eight instances in one batch under a budget that holds each alone but
+    # not all of them: growths wait for memory, when every instance waits the
+    # least advanced one starts again later, and (second call, with the final
+    # sizes of the first as hints) instances whose first buffers do not fit
+    # start when memory frees; every result is the solo one
+    probs = [vfb_b200.Problem.from_instance(i)
+             for i in cases.unsatisfiable_cases(seeds=range(4242, 4250))]
+    with vfb_b200.Engine() as eng:
+        full = [eng.solve(p) for p in probs]
+    budget = cases.smallest_solo_budget(probs, full)
+    assert budget is not None
+    key = lambda r: (r.status, r.size, r.rpn, r.level_rows, r.level_cands)  # noqa: E731
+    with vfb_b200.Engine(mem_limit_bytes=budget) as eng:
+        got = eng.batch_solve(probs)
+        again = eng.batch_solve(probs)      # with the capacity hints of the first call
+    assert [key(r) for r in got] == [key(r) for r in full]
+    assert [key(r) for r in again] == [key(r) for r in full]

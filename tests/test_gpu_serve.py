@@ -93,20 +93,11 @@ def test_oversubscribed_memory_waits_instead_of_failing():
     # budget at once: a growth that finds the memory held by the others waits
     # (or its request restarts later) instead of failing, so every result is
     # still the solo one
-    probs = []
-    for seed in (4242, 4243, 4244, 4245):
-        inst = cases.random_instance(seed, 4, 5, 5, 16, 8)
-        inst.neg[0] = inst.pos[0]          # unsatisfiable: every level up to size 8 is built
-        probs.append(vfb_b200.Problem.from_instance(inst))
+    probs = [vfb_b200.Problem.from_instance(i) for i in cases.unsatisfiable_cases()]
     with vfb_b200.Engine() as eng:
         full = [eng.solve(p) for p in probs]
     assert all(r.status == vfb_b200.NOT_FOUND for r in full)
-    budget = None   # the smallest of these budgets that holds each request alone
-    for mb in (32, 48, 64, 96, 128, 192, 256):
-        with vfb_b200.Engine(mem_limit_bytes=mb << 20) as eng:
-            if all(_key(eng.solve(p)) == _key(f) for p, f in zip(probs, full)):
-                budget = mb << 20
-                break
+    budget = cases.smallest_solo_budget(probs, full)   # holds each request alone
     assert budget is not None
     with vfb_b200.Engine(mem_limit_bytes=budget) as eng:
         # admit all four at once; no per-request cap below the device budget

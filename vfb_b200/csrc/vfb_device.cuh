@@ -42,6 +42,8 @@ enum Status : int {
   ST_NEED_MEM = 4,     // a buffer is too small: host grows it and re-runs the level
   ST_ERROR = 5,
   ST_LIMIT = 6,        // an on-the-fly level held no solution: the search cannot go on
+  ST_WAIT = 7,         // batch: memory for the next level is held by other instances; the
+                       // host retries the growth later (kernels leave the instance alone)
 };
 
 enum NeedBits : int {

@@ -37,6 +37,7 @@ struct InstHost {
   bool active = false;
   vfb_status fail = VFB_OK;
   int accounted = 1;  // last level whose bytes were added to the profile
+  bool restart = false;  // batch: evicted for memory (or never fitted): solved alone after the batch
 };
 
 uint64_t pow2_at_least(uint64_t x) {
@@ -122,6 +123,7 @@ struct Engine {
   std::map<void*, size_t> live_blocks;
   size_t held_bytes = 0;    // live + cached
   size_t cached_bytes = 0;  // blocks in free_blocks
+  size_t peak_live = 0;     // most bytes live at once since the last trim
 
   // per-call counters
   uint64_t c_h2d = 0, c_d2h = 0, c_launch = 0;
@@ -208,6 +210,7 @@ struct Engine {
       cached_bytes -= it->first;
       free_blocks.erase(it);
       live_blocks[p] = *got;
+      peak_live = std::max(peak_live, held_bytes - cached_bytes);
       return p;
     }
     // make room: drop cached blocks before exceeding the budget
@@ -222,12 +225,40 @@ struct Engine {
     void* p = nullptr;
     if (cudaMallocAsync(&p, bytes, stream) != cudaSuccess) {
       cudaGetLastError();
-      return nullptr;
+      // the device itself is full (other contexts hold the rest): give the
+      // cached blocks back to the pool and try once more
+      if (free_blocks.empty()) return nullptr;
+      for (auto& fb : free_blocks) {
+        cudaFreeAsync(fb.second, stream);
+        held_bytes -= fb.first;
+      }
+      free_blocks.clear();
+      cached_bytes = 0;
+      if (cudaMallocAsync(&p, bytes, stream) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+      }
     }
     held_bytes += bytes;
     live_blocks[p] = bytes;
     *got = bytes;
+    peak_live = std::max(peak_live, held_bytes - cached_bytes);
     return p;
+  }
+
+  // After a call: keep cached at most what the call had live at its peak (the
+  // blocks the next call of its kind reuses); the rest, superseded sizes from
+  // buffer growth, goes back to the device's memory pool, where other
+  // contexts of the process can allocate it.
+  void trim_cache() {
+    while (cached_bytes > peak_live && !free_blocks.empty()) {
+      auto big = std::prev(free_blocks.end());
+      cudaFreeAsync(big->second, stream);
+      held_bytes -= big->first;
+      cached_bytes -= big->first;
+      free_blocks.erase(big);
+    }
+    peak_live = held_bytes - cached_bytes;
   }
   void dfree(void* p) {
     if (!p) return;
@@ -255,7 +286,17 @@ struct Engine {
     sms = prop.multiProcessorCount;
     size_t freeb = 0, total = 0;
     cudaMemGetInfo(&freeb, &total);
-    mem_limit = (o && o->mem_limit_bytes) ? o->mem_limit_bytes : (size_t)(0.9 * (double)freeb);
+    // memory the process's pool holds but has not handed out is available too
+    size_t pool_spare = 0;
+    {
+      cudaMemPool_t dp;
+      uint64_t reserved = 0, used = 0;
+      if (cudaDeviceGetDefaultMemPool(&dp, device) == cudaSuccess &&
+          cudaMemPoolGetAttribute(dp, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+          cudaMemPoolGetAttribute(dp, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess && reserved > used)
+        pool_spare = (size_t)(reserved - used);
+    }
+    mem_limit = (o && o->mem_limit_bytes) ? o->mem_limit_bytes : (size_t)(0.9 * (double)(freeb + pool_spare));
     if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) return VFB_DEVICE_ERROR;
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
@@ -872,7 +913,7 @@ struct Engine {
   vfb_status upload_atoms(const vfb_instance* ins, std::vector<InstHost>& H, int n) {
     size_t words = 0;
     for (int i = 0; i < n; ++i)
-      if (H[i].active) words += (size_t)H[i].d.A * H[i].d.TP;
+      if (H[i].active && H[i].d.rows) words += (size_t)H[i].d.A * H[i].d.TP;
     if (words > h_stage_words) {
       if (h_stage) cudaFreeHost(h_stage);
       h_stage = nullptr;
@@ -882,7 +923,7 @@ struct Engine {
     }
     size_t o = 0;
     for (int i = 0; i < n; ++i) {
-      if (!H[i].active) continue;
+      if (!H[i].active || !H[i].d.rows) continue;   // (not started yet: no buffers)
       const InstDev& d = H[i].d;
       uint64_t* dst = h_stage + o;
       for (int v = 0; v < d.A; ++v) {
@@ -990,13 +1031,23 @@ struct Engine {
     for (int i = 0; i < n; ++i) {
       if (H[i].fail != VFB_OK) continue;
       const InstDev& d = H[i].d;
-      Caps c = clusters ? Caps{1u << 15, 1u << 16, 1u << 16, 1u << 16} : Caps{4096, 1u << 14, 1u << 14, 1u << 13};
-      c.rows = std::max<uint64_t>(c.rows, (uint64_t)d.A * 16);
+      Caps c0 = clusters ? Caps{1u << 15, 1u << 16, 1u << 16, 1u << 16} : Caps{4096, 1u << 14, 1u << 14, 1u << 13};
+      c0.rows = std::max<uint64_t>(c0.rows, (uint64_t)d.A * 16);
+      Caps c = c0;
       H[i].sig = signature(ins[i]);
       auto hit = hints.find(H[i].sig);
       if (hit != hints.end()) c = hit->second;
-      const vfb_status s = alloc_buffers(H[i], c.rows, c.slots, c.words, c.tents);
+      vfb_status s = alloc_buffers(H[i], c.rows, c.slots, c.words, c.tents);
+      // the final sizes of an earlier solve do not all fit at once: start small
+      if (s == VFB_OOM && hit != hints.end()) s = alloc_buffers(H[i], c0.rows, c0.slots, c0.words, c0.tents);
       H[i].d.promote_above = clusters ? kPromoteAbove : ~0ULL;
+      if (s == VFB_OOM && n > 1 && !clusters) {
+        // the instances before it hold the memory: it is solved alone after them
+        H[i].d.status = ST_IDLE;
+        H[i].active = true;
+        H[i].restart = true;
+        continue;
+      }
       if (s != VFB_OK) { H[i].fail = s; H[i].d.status = ST_IDLE; continue; }
       H[i].active = true;
       chunk_need += (H[i].d.bitmap_words + kCompactWords - 1) / kCompactWords;
@@ -1034,12 +1085,31 @@ struct Engine {
     while (rc == VFB_OK) {
       if (!first) {
         bool running = false, grew = false;
+        std::vector<int> waiting;
+        int nrun = 0;
+        for (int i = 0; i < n; ++i)
+          if (H[i].active && h_status[i].x == ST_RUNNING) ++nrun;
         for (int i = 0; i < n; ++i) {
           if (!H[i].active) continue;
           const int st = h_status[i].x;
           if (st == ST_RUNNING) running = true;
-          if (st == ST_NEED_MEM) {
+          if (st == ST_NEED_MEM || st == ST_WAIT) {
             vfb_status g = grow(H[i], i);
+            // buffers of instances that are done are not needed any more
+            if (g == VFB_OOM && reclaim_finished(H, n)) g = grow(H[i], i);
+            if (g == VFB_OOM && (nrun > 0 || grew || held_by_others(H, n, i))) {
+              // the memory is held by other instances: this one waits (with
+              // whatever part did grow) and tries again when the device loop
+              // returns, at the latest when the others are done
+              InstDev& d = H[i].d;
+              d.status = ST_WAIT;
+              if (cudaMemcpyAsync(dInst + i, &d, sizeof(InstDev), cudaMemcpyHostToDevice, stream) != cudaSuccess)
+                rc = dev_fail(__LINE__);
+              c_h2d += sizeof(InstDev);
+              h_status[i].x = ST_WAIT;
+              waiting.push_back(i);
+              continue;
+            }
             if (g == VFB_OOM && !H[i].d.on_the_fly) {
               // the level's rows do not fit the budget: test its candidates as
               // solutions without storing them (LTL_BS onTheFly)
@@ -1068,6 +1138,23 @@ struct Engine {
             }
           }
           if (st == ST_ERROR) { H[i].fail = VFB_DEVICE_ERROR; H[i].active = false; }
+        }
+        if (rc != VFB_OK) break;
+        const bool pressure = !waiting.empty();
+        if (!running && pressure) {
+          // every instance with buffers waits for memory the others hold:
+          // the least advanced one gives its buffers up and is solved alone
+          // after the others (its result is the same, only later)
+          int v = waiting[0];
+          for (int i : waiting)
+            if (H[i].d.level <= H[v].d.level) v = i;
+          free_buffers(H[v]);
+          H[v].restart = true;
+          const int idle = ST_IDLE;
+          cudaMemcpyAsync(&dInst[v].status, &idle, sizeof(int), cudaMemcpyHostToDevice, stream);
+          c_h2d += sizeof(int);
+          h_status[v].x = ST_IDLE;
+          running = true;   // the others retry their growth on the next pass
         }
         if (!running || rc != VFB_OK) break;
         if (grew) {
@@ -1100,7 +1187,9 @@ struct Engine {
       }
       if (profile) profile_step(n, H);
       if (verbose) report_progress(n);
-      if (++guard > 64 * kMaxSize) { rc = dev_fail(__LINE__); break; }
+      // (a bound on host passes: every level and growth of every instance, with
+      // room for the waits and restarts of a batch under memory pressure)
+      if (++guard > 64 * kMaxSize * std::max(1, n)) { rc = dev_fail(__LINE__); break; }
     }
     // results
     std::vector<InstDev> recs(n);
@@ -1174,14 +1263,56 @@ struct Engine {
       }
     }
     for (int i = 0; i < n; ++i) {
-      if (!H[i].d.rows) continue;
-      if (recs[i].status == ST_FOUND || recs[i].status == ST_NOT_FOUND) {
+      // (an instance whose buffers were reclaimed during the call has its
+      // final capacities in its record all the same)
+      if (H[i].fail == VFB_OK && (recs[i].status == ST_FOUND || recs[i].status == ST_NOT_FOUND)) {
         if (hints.size() > 4096) hints.clear();
         hints[H[i].sig] = Caps{recs[i].row_cap, recs[i].table_mask + 1, recs[i].bitmap_words, recs[i].tent_cap};
       }
-      free_buffers(H[i]);
+      if (H[i].d.rows) free_buffers(H[i]);
+    }
+    trim_cache();
+    // evicted instances, and ones whose first buffers did not fit, are solved
+    // alone now that the others' buffers are free
+    if (rc == VFB_OK) {
+      std::vector<int> later;
+      for (int i = 0; i < n; ++i)
+        if (H[i].restart) later.push_back(i);
+      for (int i : later) {
+        vfb_result r;
+        const vfb_status s = batch(&ins[i], 1, &r);
+        out[i] = r;
+        if (s != VFB_OK) out[i].status = s;
+      }
     }
     return rc;
+  }
+
+  // Frees the buffers of instances whose search is over (their results are in
+  // their device records); returns whether anything was freed.  Not while a
+  // BS stage is to follow: it reads the cached rows.
+  // Whether an instance other than i still holds buffers and has not finished.
+  bool held_by_others(const std::vector<InstHost>& H, int n, int i) const {
+    for (int j = 0; j < n; ++j) {
+      if (j == i || !H[j].d.rows) continue;
+      const int st = h_status[j].x;
+      if (st == ST_RUNNING || st == ST_NEED_MEM || st == ST_WAIT) return true;
+    }
+    return false;
+  }
+
+  bool reclaim_finished(std::vector<InstHost>& H, int n) {
+    if (bs_max > 0) return false;
+    bool any = false;
+    for (int j = 0; j < n; ++j) {
+      if (!H[j].d.rows) continue;
+      const int st = h_status[j].x;
+      if (st == ST_FOUND || st == ST_NOT_FOUND || st == ST_LIMIT) {
+        free_buffers(H[j]);
+        any = true;
+      }
+    }
+    return any;
   }
 
   void report_progress(int n) {
@@ -1280,6 +1411,7 @@ struct Engine {
       if (sv.busy[i] && sv.H[i].d.rows) free_buffers(sv.H[i]);
     if (sv.h_inst) cudaFreeHost(sv.h_inst);
     sv = Session{};
+    trim_cache();
     single_step = false;
     if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
   }
