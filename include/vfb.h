@@ -103,7 +103,11 @@ void vfb_destroy(void *ctx);
  * otherwise the call ends with VFB_LIMIT and the sizes it stored. */
 vfb_status vfb_solve(void *ctx, const vfb_instance *inst, vfb_result *out);
 
-/* Solves n independent instances together; out[i] equals vfb_solve(inst[i]). */
+/* Solves n independent instances together; out[i] equals vfb_solve(inst[i])
+ * under the same memory budget.  When the budget cannot hold every instance
+ * at once, instances wait for memory the others free, and an instance that
+ * cannot get its buffers while the others hold theirs is solved alone after
+ * them. */
 vfb_status vfb_batch_solve(void *ctx, const vfb_instance *inst, int n, vfb_result *out);
 
 /* vfb_solve with the operator costs of LTL_BS (LTLI LTL_BS.cu:1069-1532,
