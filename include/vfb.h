@@ -54,7 +54,9 @@ typedef enum {
 
 typedef struct {
   int device;              /* CUDA device ordinal */
-  size_t mem_limit_bytes;  /* device memory budget of one solve/batch (0: 90% of free memory) */
+  size_t mem_limit_bytes;  /* device memory budget of one solve/batch (0: 90% of the memory
+                              free at creation, counting what the process's stream-ordered
+                              pool holds unused) */
   int verbose;             /* 1: per-level progress lines on stderr */
   int profile;             /* 1: time every kernel of the level step with CUDA events
                               (see vfb_profile_read); adds one event pair per kernel */
