@@ -79,3 +79,29 @@ def smallest_solo_budget(probs, want, sizes_mb=(32, 48, 64, 96, 128, 192, 256)):
             if all(key(eng.solve(p)) == key(w) for p, w in zip(probs, want)):
                 return mb << 20
     return None
+
+
+def mirrored_cases(count: int = 8, num_vars: int = 5, length: int = 18, max_size: int = 6):
+    """Instances whose relaxed (hash) keys collide for every formula and its
+    mirror (propositions 0 and 1 swapped): traces come in pairs, the second
+    the first with propositions 0 and 1 exchanged, both in the same half of the
+    traces (hash keys fold each half with XOR, so the pair's words cancel
+    into the same key).  Traces 0, 1 are positive and their mirrors 2, 3
+    negative, so a formula and its mirror never both solve: whenever the
+    first solving formula's mirror comes earlier in the order, the first
+    solving candidate does not own its key."""
+    out = []
+    for s in range(count):
+        rng = synth.Rng(7000 + s)
+        base = [[rng.bernoulli_word(length, 0.5) for _ in range(num_vars)] for _ in range(4)]
+        def mirror(w):
+            m = list(w)
+            m[0], m[1] = w[1], w[0]
+            return m
+        # halves of 8 traces: {0, 1, 2, 3} and {4, 5, 6, 7}
+        traces = [base[0], base[1], mirror(base[0]), mirror(base[1]),
+                  base[2], mirror(base[2]), base[3], mirror(base[3])]
+        tr = [(length, w) for w in traces]
+        out.append(synth.Instance(num_vars, tr[:2], tr[2:], max_size,
+                                  [f"p{v}" for v in range(num_vars)], None, 3, f"mirror{s}"))
+    return out

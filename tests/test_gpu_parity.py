@@ -203,3 +203,21 @@ def test_batch_under_memory_pressure_equals_solo():
         again = eng.batch_solve(probs)      # with the capacity hints of the first call
     assert [key(r) for r in got] == [key(r) for r in full]
     assert [key(r) for r in again] == [key(r) for r in full]
+
+
+@pytest.mark.parametrize("inst", cases.mirrored_cases() + cases.mirrored_cases(count=8, num_vars=8, length=20,
+                                                                               max_size=7),
+                         ids=lambda i: f"{i.name}_a{i.num_vars}")
+def test_relaxed_key_collisions_on_the_solution(engine, inst):
+    # the first solving candidate often shares its hash key with its earlier
+    # mirror (which does not solve); candidates past it may have been skipped
+    # by then, so the level is built again in full before the answer is read
+    _check(engine, inst)
+
+
+def test_relaxed_key_collisions_in_a_batch(engine):
+    insts = cases.mirrored_cases(count=8, num_vars=8, length=20, max_size=7) + cases.mirrored_cases()
+    probs = [vfb_b200.Problem.from_instance(i) for i in insts]
+    key = lambda r: (r.status, r.size, r.rpn, r.level_rows, r.level_cands, r.solution_index)  # noqa: E731
+    solo = [engine.solve(p) for p in probs]
+    assert [key(r) for r in engine.batch_solve(probs)] == [key(r) for r in solo]

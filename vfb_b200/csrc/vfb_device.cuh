@@ -115,6 +115,13 @@ struct InstDev {
   // group g: kind 0 = unary over level la (mask bits ~ X F G), kind 1 = binary
   // over levels la <= lb (mask bits &, |, la U lb, lb U la)
   uint8_t grp_kind[kGroups], grp_mask[kGroups], grp_la[kGroups], grp_lb[kGroups];
+  // first candidate index of each operator of a group: unary ~ X F G at
+  // operand row 0, binary & | laUlb lbUla at operand rows (0, 0)
+  uint64_t grp_base[kGroups][4];
+  int p1_masked;   // a P1 tile of this attempt skipped operators past best_cand
+  int no_mask;     // this level is re-run without skipping (set by the table scan)
+  int mask_off;    // never skip (contexts that cannot re-run a level)
+  int pad_m;
   int ngroups;
   int tq;                      // staged rows per P1 tile at this level (1..kTQ)
   int p1_blocks;               // P1 CTAs this level asks for (0: every resident CTA)

@@ -439,7 +439,7 @@ struct Engine {
     if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
     // one thread per instance (whole warps, at most 1024): small batches keep
     // k_advance's block scans short
-    adv_threads = std::min(1024, std::max(32, (ninst + 31) / 32 * 32));
+    adv_threads = std::min(kAdvanceThreads, std::max(32, (ninst + 31) / 32 * 32));
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaGraphCreate(&graph, 0);
     if (e != cudaSuccess) return e;

@@ -67,19 +67,21 @@ __device__ void plan_one(InstDev& I) {
   // cost c reads level k - c, & | over splits (i, k - c - i) with i <= k - c - i,
   // U over every split (LTL_BS.cu:1226-1488; unit costs: the size order)
   uint64_t g = 0;
+  uint64_t bA[kMaxSize + 1], bO[kMaxSize + 1], bU[kMaxSize + 1];   // block bases by left level
   I.base_not = g;
   if (Ln >= 0) g += n[Ln];
   for (int pass = 0; pass < 2; ++pass) {
     const int w = pass ? wO : wA;
     for (int i = c1; 2 * i <= k - w; ++i) {
       const int j = k - w - i;
+      (pass ? bO : bA)[i] = g;
       (pass ? I.base_or : I.base_and)[i] = g;
       g += n[i] * n[j];
     }
   }
+  uint64_t bx[3];
   {
     const int ws[3] = {wX, wF, wG};
-    uint64_t bx[3];
 #pragma unroll
     for (int o = 0; o < 3; ++o) {
       const int L = k - ws[o];
@@ -91,6 +93,7 @@ __device__ void plan_one(InstDev& I) {
     I.base_g = bx[2];
   }
   for (int i = c1; k - wU - i >= c1; ++i) {
+    bU[i] = g;
     I.base_u[i] = g;
     g += n[i] * n[k - wU - i];
   }
@@ -167,6 +170,28 @@ __device__ void plan_one(InstDev& I) {
     for (int q = 0; q < ng; ++q) add_tiles(I.grp_kind[q], I.grp_la[q], I.grp_lb[q]);
   }
   I.ngroups = ng;
+  // operator bases of every group (what a P1 tile needs to tell whether an
+  // operator's candidates can still come before the best solution found)
+  for (int q = 0; q < ng; ++q) {
+    const int kind = weighted ? I.grp_kind[q] : (q > 0);
+    const int mask = weighted ? I.grp_mask[q] : (q == 0 ? 0xF : (2 * q == k - 1 ? 7 : 15));
+    const int la = weighted ? I.grp_la[q] : (q ? q : k - 1);
+    const int lb = weighted ? I.grp_lb[q] : (q ? k - 1 - q : 0);
+    uint64_t b4[4];
+    if (kind == 0) {
+      b4[0] = 0;   // ~ is the first block
+      b4[1] = bx[0];
+      b4[2] = bx[1];
+      b4[3] = bx[2];
+    } else {
+      b4[0] = (mask & 1) ? bA[la] : 0;
+      b4[1] = (mask & 2) ? bO[la] : 0;
+      b4[2] = (mask & 4) ? bU[la] : 0;
+      b4[3] = (mask & 8) ? bU[lb] : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) I.grp_base[q][u] = b4[u];
+  }
   // P1 tiling: kTS stream rows x tq staged rows per tile.  The staged height
   // is the largest power of two within the band's bound whose tile count
   // reaches the band's target (small levels get shorter tiles so that they
@@ -230,6 +255,8 @@ __device__ void plan_one(InstDev& I) {
     I.n_new = I.n_wins = I.probe_fail = I.n_newlist = 0;
     I.best_cand = I.best_sol = ~0ULL;
     I.sol_known = 0;
+    I.p1_masked = 0;
+    if (attempt_level != k) I.no_mask = 0;   // a new level may skip again
     I.attempt = (attempt_level == k) ? attempt + 1 : 1;
     I.attempt_level = k;
   }
@@ -318,6 +345,11 @@ __device__ void ph_p1(const BatchDev& B) {
           const int i = __ldcg(&Ip->grp_la[grp]), j = __ldcg(&Ip->grp_lb[grp]);
           const uint64_t ni = __ldcg(&Ip->lcount[i]), nj = kind ? __ldcg(&Ip->lcount[j]) : 0;
           const uint64_t qt = kind ? __ldcg(&Ip->grp_qtiles[grp]) : 1;
+          const unsigned long long best = __ldcg(&Ip->best_cand);
+          const int may_skip = !__ldcg(&Ip->no_mask) && !__ldcg(&Ip->mask_off);
+          uint64_t gb[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) gb[u] = __ldcg(&Ip->grp_base[grp][u]);
           const uint64_t within = local - gstart;
           P.inst = b;
           P.grp = grp;
@@ -334,11 +366,19 @@ __device__ void ph_p1(const BatchDev& B) {
           P.otf = __ldcg(&Ip->on_the_fly);
           P.skip = !P.otf && ((fails != 0) || (4 * (keys + fresh) > 3 * cap));
           P.kind = kind;
-          P.mask = gmask;
+          // operators whose first candidate in this tile comes after the best
+          // solution candidate found so far cannot change the result (every
+          // candidate before it is still evaluated): they are skipped
+          unsigned keep = 0xF;
           if (kind == 0) {
             P.si = i;
             P.nS = ni;
             P.s0 = within * kTS;
+            if (may_skip && best != ~0ULL) {
+              keep = 0;
+#pragma unroll
+              for (int u = 0; u < 4; ++u) keep |= (gb[u] + P.s0 <= best ? 1u : 0u) << u;
+            }
           } else {
             const int qleft = (i == j) || (ni <= nj);
             P.i = i;
@@ -354,7 +394,15 @@ __device__ void ph_p1(const BatchDev& B) {
             divmod64(within, qt, sq, qr);
             P.s0 = sq * kTS;
             P.q0 = qr * tq;
+            if (may_skip && best != ~0ULL) {
+              const uint64_t amin = qleft ? P.q0 : P.s0, bmin = qleft ? P.s0 : P.q0;
+              const uint64_t ab = amin * nj + bmin;
+              keep = (gb[0] + ab <= best ? 1u : 0u) | (gb[1] + ab <= best ? 2u : 0u) |
+                     (gb[2] + ab <= best ? 4u : 0u) | (gb[3] + bmin * ni + amin <= best ? 8u : 0u);
+            }
           }
+          P.mask = gmask & keep;
+          if (P.mask != gmask) *(volatile int*)&const_cast<InstDev*>(Ip)->p1_masked = 1;
         }
       }
     }
@@ -370,7 +418,9 @@ __device__ void ph_p1(const BatchDev& B) {
     uint64_t* sS = smem;
     uint64_t* sQ = smem + kTS * sp;
     P1Count cnt{0, 0, ~0ULL};
-    if (!P.skip) {
+    // a tile whose every operator is skipped has nothing to do
+    const bool idle = P.skip || (!P.otf && P.mask == 0);
+    if (!idle) {
       const int ns = (int)((P.nS - P.s0) < (uint64_t)kTS ? (P.nS - P.s0) : (uint64_t)kTS);
       stage_rows(sS, sp, row_ptr(I, P.si, P.s0), ns, P.TP);
       if (P.kind == 1) {
@@ -380,25 +430,23 @@ __device__ void ph_p1(const BatchDev& B) {
       stage_wait();
     }
     __syncthreads();
-    if (!P.skip && P.otf) {
+    if (!idle && P.otf) {
       p1_solutions(I, P, sS, sp, sQ, cnt);
-    } else if (!P.skip) {
-      const bool four = P.kind == 1 && (P.mask & 8);
+    } else if (!idle) {
+      // binary tiles compute the operators up to the last one kept (& | laUlb lbUla)
+      const int keys = (P.mask & 8) ? 15 : (P.mask & 4) ? 7 : 3;
       switch (P.mode) {
         case KEY_HASH:
           if (P.kind == 0) p1_unary<KEY_HASH>(I, P, sS, sp, cnt);
-          else if (four) p1_binary<KEY_HASH, true>(I, P, sS, sp, sQ, cnt);
-          else p1_binary<KEY_HASH, false>(I, P, sS, sp, sQ, cnt);
+          else p1_binary_keys<KEY_HASH>(keys, I, P, sS, sp, sQ, cnt);
           break;
         case KEY_SAMPLED:
           if (P.kind == 0) p1_unary<KEY_SAMPLED>(I, P, sS, sp, cnt);
-          else if (four) p1_binary<KEY_SAMPLED, true>(I, P, sS, sp, sQ, cnt);
-          else p1_binary<KEY_SAMPLED, false>(I, P, sS, sp, sQ, cnt);
+          else p1_binary_keys<KEY_SAMPLED>(keys, I, P, sS, sp, sQ, cnt);
           break;
         default:
           if (P.kind == 0) p1_unary<KEY_CONCAT>(I, P, sS, sp, cnt);
-          else if (four) p1_binary<KEY_CONCAT, true>(I, P, sS, sp, sQ, cnt);
-          else p1_binary<KEY_CONCAT, false>(I, P, sS, sp, sQ, cnt);
+          else p1_binary_keys<KEY_CONCAT>(keys, I, P, sS, sp, sQ, cnt);
       }
     }
     // per-tile counter flush: warp reductions, then one atomic per counter
@@ -508,9 +556,19 @@ __device__ void ph_table_scan(const BatchDev& B, unsigned bid, unsigned nb) {
       case KEY_SAMPLED: warp_key<KEY_SAMPLED>(I, cd, lane, h, l); break;
       default: warp_key<KEY_CONCAT>(I, cd, lane, h, l);
     }
-    if (lane == 0 && find_pay(I.table, I.table_mask, h, l) == pay_of(k, g)) {
-      I.best_sol = g;
-      I.sol_known = 1;
+    if (lane == 0) {
+      if (find_pay(I.table, I.table_mask, h, l) == pay_of(k, g)) {
+        I.best_sol = g;
+        I.sol_known = 1;
+      } else if (I.p1_masked) {
+        // an earlier candidate of the level shares the first solution's key
+        // (a relaxed-key collision) while operators past it were skipped: the
+        // level is built again in full (the host re-plans it, nothing to grow)
+        I.no_mask = 1;
+        I.need = 0;
+        I.planned = 0;
+        I.status = ST_NEED_MEM;
+      }
     }
   }
 }
@@ -842,7 +900,7 @@ __global__ void k_finish(BatchDev* Bp) {
 // instance not yet planned for its current level is planned.  The batch's
 // tile and chunk prefixes are rebuilt from the recorded plans, the
 // look-back states of k_compact cleared and the work tickets reset.
-__global__ void __launch_bounds__(1024) k_advance(BatchDev* Bp, cudaGraphConditionalHandle handle, int built,
+__global__ void __launch_bounds__(kAdvanceThreads) k_advance(BatchDev* Bp, cudaGraphConditionalHandle handle, int built,
                                                   int loop, unsigned int max_iter) {
   __shared__ int s_run, s_need;
   __shared__ unsigned s_blocks;

@@ -11,6 +11,9 @@ constexpr int kScanSlots = 8192;      // hash-set slots per table-scan chunk
 constexpr int kScanBatch = 8;         // table-scan entries a thread reads at a time
 constexpr int kCompactWords = 512;    // owner-bitmap words per k_compact chunk (16384 candidates)
 constexpr int kCompactThreads = 256;  // threads per k_compact CTA (two bitmap words each)
+// k_advance threads at most (it loops over larger batches): few enough that
+// the one-thread plan and finish keep their state in registers
+constexpr int kAdvanceThreads = 256;
 constexpr int kTickets = 8;            // words of BatchDev::tickets
 constexpr int kTicketP1Blocks = 4;     // tickets[4]: CTAs the step's k_p1 runs (0: all), set by k_advance
 constexpr int kEmitGroup = 4;         // owners per warp step of k_emit

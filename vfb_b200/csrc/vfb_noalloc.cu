@@ -86,6 +86,7 @@ struct Carver {
 // key layout of LTL_BS.cu:30-110).
 vfb_status fill_problem(const vfb_instance& in, InstDev& d) {
   std::memset(&d, 0, sizeof(d));
+  d.mask_off = 1;   // no level re-runs here: P1 never skips operators
   const int T = in.num_traces, A = in.num_vars;
   if (T < 1 || T > kMaxTraces || A < 1 || A > VFB_MAX_VARS || in.num_pos < 0 || in.num_pos > T)
     return VFB_LIMIT;

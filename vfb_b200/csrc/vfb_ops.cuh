@@ -465,9 +465,13 @@ __device__ inline void p1_unary(InstDev& I, const TileSh& P, const uint64_t* sS,
   insert_group<4>(I, live, P.k, h, l, g, bad, cnt, (unsigned)P.mask);
 }
 
-template <int MODE, bool FOUR>
+// KEYS: the operators computed, a prefix of (&, |, laUlb, lbUla) as bits
+// 3, 7, 15; the inserted ones are P.mask within it.
+template <int MODE, int KEYS>
 __device__ inline void p1_binary(InstDev& I, const TileSh& P, const uint64_t* sS, int sp, const uint64_t* sQ,
                           P1Count& cnt) {
+  constexpr bool kO = (KEYS & 2) != 0, kU = (KEYS & 4) != 0, kV = (KEYS & 8) != 0;
+  constexpr int N = 1 + (kO ? 1 : 0) + (kU ? 1 : 0) + (kV ? 1 : 0);
   const uint64_t s = P.s0 + threadIdx.x;
   const unsigned live = __ballot_sync(0xffffffffu, s < P.nS);
   if (s >= P.nS) return;
@@ -475,8 +479,11 @@ __device__ inline void p1_binary(InstDev& I, const TileSh& P, const uint64_t* sS
   const int nq = (int)((P.nQ - P.q0) < (uint64_t)P.tq ? (P.nQ - P.q0) : (uint64_t)P.tq);
   for (int q = 0; q < nq; ++q) {
     const uint64_t* qrow = sQ + q * P.TP;
-    KeyAcc kA, kO, kU, kV;
-    key_init(kA); key_init(kO); key_init(kU); key_init(kV);
+    KeyAcc kA, kOr, kUn, kVn;
+    key_init(kA);
+    if (kO) key_init(kOr);
+    if (kU) key_init(kUn);
+    if (kV) key_init(kVn);
     uint32_t bad[4] = {0, 0, 0, 0};
     auto body = [&](int t, auto half) {
       constexpr bool HI = decltype(half)::hi;
@@ -484,40 +491,51 @@ __device__ inline void p1_binary(InstDev& I, const TileSh& P, const uint64_t* sS
       const uint64_t la = P.qleft ? qw : sw, lb = P.qleft ? sw : qw;
       const int L = P.len[t], off = P.off[t], wd = P.wid[t];
       const uint32_t pb = (uint32_t)pos_bit(P, t);
-      const uint64_t wa = la & lb, wo = la | lb, wu = w_until(la, lb);
+      const uint64_t wa = la & lb;
       bad[0] |= lo32(wa) ^ pb;
-      bad[1] |= lo32(wo) ^ pb;
-      bad[2] |= lo32(wu) ^ pb;
       key_word_h<MODE, HI>(kA, wa, t, off, wd, P.stride, L);
-      key_word_h<MODE, HI>(kO, wo, t, off, wd, P.stride, L);
-      key_word_h<MODE, HI>(kU, wu, t, off, wd, P.stride, L);
-      if (FOUR) {
+      if (kO) {
+        const uint64_t wo = la | lb;
+        bad[1] |= lo32(wo) ^ pb;
+        key_word_h<MODE, HI>(kOr, wo, t, off, wd, P.stride, L);
+      }
+      if (kU) {
+        const uint64_t wu = w_until(la, lb);
+        bad[2] |= lo32(wu) ^ pb;
+        key_word_h<MODE, HI>(kUn, wu, t, off, wd, P.stride, L);
+      }
+      if (kV) {
         const uint64_t wv = w_until(lb, la);
         bad[3] |= lo32(wv) ^ pb;
-        key_word_h<MODE, HI>(kV, wv, t, off, wd, P.stride, L);
+        key_word_h<MODE, HI>(kVn, wv, t, off, wd, P.stride, L);
       }
     };
     for (int t = 0; t < P.half; ++t) body(t, Half<true>{});
     for (int t = P.half; t < P.T; ++t) body(t, Half<false>{});
     const uint64_t a = P.qleft ? P.q0 + q : s;     // index in level i
     const uint64_t b = P.qleft ? s : P.q0 + q;     // index in level j
+    const uint64_t ab = a * P.nj + b;
     uint64_t h[4], l[4], g[4];
     key_final<MODE>(kA, h[0], l[0]);
-    key_final<MODE>(kO, h[1], l[1]);
-    key_final<MODE>(kU, h[2], l[2]);
-    const uint64_t ab = a * P.nj + b;
     g[0] = I.base_and[P.i] + ab;
-    g[1] = I.base_or[P.i] + ab;
-    g[2] = I.base_u[P.i] + ab;
+    if (kO) { key_final<MODE>(kOr, h[1], l[1]); g[1] = I.base_or[P.i] + ab; }
+    if (kU) { key_final<MODE>(kUn, h[2], l[2]); g[2] = I.base_u[P.i] + ab; }
+    if (kV) { key_final<MODE>(kVn, h[3], l[3]); g[3] = I.base_u[P.j] + b * P.ni + a; }
 #pragma unroll
     for (int j = 0; j < 4; ++j) bad[j] &= 1u;
-    if (FOUR) {
-      key_final<MODE>(kV, h[3], l[3]);
-      g[3] = I.base_u[P.j] + b * P.ni + a;
-      insert_group<4>(I, live, P.k, h, l, g, bad, cnt, (unsigned)P.mask);
-    } else {
-      insert_group<3>(I, live, P.k, h, l, g, bad, cnt, (unsigned)P.mask & 7u);
-    }
+    insert_group<N>(I, live, P.k, h, l, g, bad, cnt, (unsigned)P.mask & (unsigned)KEYS);
+  }
+}
+
+template <int MODE>
+__device__ inline void p1_binary_keys(int keys, InstDev& I, const TileSh& P, const uint64_t* sS, int sp,
+                                      const uint64_t* sQ, P1Count& cnt) {
+  switch (keys) {
+    case 15: p1_binary<MODE, 15>(I, P, sS, sp, sQ, cnt); break;
+    case 7: p1_binary<MODE, 7>(I, P, sS, sp, sQ, cnt); break;
+    // & alone is computed with | (one variant less: a smaller kernel image
+    // measured faster on small levels)
+    default: p1_binary<MODE, 3>(I, P, sS, sp, sQ, cnt);
   }
 }
 
