@@ -221,3 +221,21 @@ def test_relaxed_key_collisions_in_a_batch(engine):
     key = lambda r: (r.status, r.size, r.rpn, r.level_rows, r.level_cands, r.solution_index)  # noqa: E731
     solo = [engine.solve(p) for p in probs]
     assert [key(r) for r in engine.batch_solve(probs)] == [key(r) for r in solo]
+
+
+def test_relaxed_key_collisions_with_tiles_in_order():
+    # one CTA takes the tiles in order, so every tile after the first
+    # solution's skips the operators past it; where that solution turns out
+    # not to own its key, the level is built again in full (this set has
+    # several such levels) and the answer still equals the oracle's
+    insts = cases.mirrored_cases() + cases.mirrored_cases(count=8, num_vars=8, length=20, max_size=7)
+    insts += cases.mirrored_cases(count=24, num_vars=12, length=16, max_size=7)[8:]
+    with vfb_b200.Engine() as eng:
+        eng.set_tune({"rows": [1] * vfb_b200.TUNE_BANDS, "tiles_log2": [16] * vfb_b200.TUNE_BANDS,
+                      "blocks": [1] * vfb_b200.TUNE_BANDS})
+        for inst in insts:
+            got = eng.solve(vfb_b200.Problem.from_instance(inst))
+            ref = oracle.solve(oracle.Problem.from_instance(inst))
+            assert got.rpn == ref["rpn"], inst.name
+            assert got.level_rows == ref["level_rows"], inst.name
+            assert got.level_cands == ref["level_cands"], inst.name
