@@ -40,6 +40,13 @@ struct InstHost {
   bool restart = false;  // batch: evicted for memory (or never fitted): solved alone after the batch
 };
 
+// Serving: a request whose first buffers are at most this large is admitted
+// past the projected budget when they fit what is actually free.
+constexpr uint64_t kLightRequestBytes = 256ull << 20;
+// Serving: two or more requests waiting for memory this many steps running
+// count as a deadlock (the least advanced one is evicted).
+constexpr int kServeWaitSteps = 32;
+
 uint64_t pow2_at_least(uint64_t x) {
   uint64_t p = 1;
   while (p < x) p <<= 1;
@@ -1347,6 +1354,7 @@ struct Engine {
     std::deque<Pending> queue;
     std::vector<uint64_t> proj;   // projected bytes of each busy slot after its next level
     std::vector<Pending> req;     // the request each busy slot holds (requeued if it is evicted)
+    std::vector<int> waited;      // consecutive steps each busy slot has waited for memory
     uint64_t evictions = 0;       // requests evicted and queued again (memory held by the others)
     InstDev* h_inst = nullptr;    // pinned mirror of the slot records
     int p1_smem = 0;
@@ -1382,6 +1390,7 @@ struct Engine {
     sv.proj.assign(slots, 0);
     sv.req.clear();
     sv.req.resize(slots);
+    sv.waited.assign(slots, 0);
     sv.budget_frac = sv_budget_frac;
     sv.request_bytes = sv_request_bytes ? sv_request_bytes : (uint64_t)(mem_limit / 4);
     sv.step_cands = sv_step_cands;
@@ -1475,9 +1484,12 @@ struct Engine {
     for (int i = 0; i < sv.cap; ++i)
       if (sv.busy[i]) { committed += sv.proj[i]; ++nbusy; }
     const double budget = sv.budget_frac * (double)mem_limit;
+    const uint64_t live = held_bytes - cached_bytes;
     for (int i = 0; i < sv.cap && !sv.queue.empty(); ++i) {
       if (sv.busy[i]) continue;
-      if (mem_limit && nbusy > 0 && (double)committed > budget) break;
+      // past the projected budget only a light request still goes in, when
+      // its first buffers fit the memory budget beside what is live now
+      const bool over = mem_limit && nbusy > 0 && (double)committed > budget;
       Pending& p = sv.queue.front();
       InstHost& H = sv.H[i];
       H = InstHost{};
@@ -1493,6 +1505,13 @@ struct Engine {
           const Caps& h = hit->second;
           const uint64_t hb = h.rows * ((uint64_t)H.d.TP * 8 + 8) + h.slots * sizeof(Slot) + h.words * 4 + h.tents * 8;
           if (hb <= sv.request_bytes) c = h;
+        }
+        if (over) {
+          const uint64_t cb = c.rows * ((uint64_t)H.d.TP * 8 + 8) + c.slots * sizeof(Slot) + c.words * 4 + c.tents * 8;
+          if (cb > kLightRequestBytes || live + cb > mem_limit) {
+            H = InstHost{};
+            break;
+          }
         }
         s = alloc_buffers(H, c.rows, c.slots, c.words, c.tents);
         if (s == VFB_OOM && nbusy > 0) {
@@ -1580,6 +1599,7 @@ struct Engine {
             return dev_fail(__LINE__);
           c_h2d += sizeof(InstDev);
           waiting.push_back(i);
+          ++sv.waited[i];
         } else if (g != VFB_OK) {
           sv.H[i].fail = g;
           const int err = ST_ERROR;
@@ -1587,6 +1607,7 @@ struct Engine {
           fin.push_back(i);
         } else {
           progress = true;
+          sv.waited[i] = 0;
         }
       } else if (st == ST_FOUND || st == ST_NOT_FOUND || st == ST_ERROR || st == ST_LIMIT) {
         fin.push_back(i);
@@ -1594,7 +1615,12 @@ struct Engine {
         progress = true;
       }
     }
-    if (!progress && fin.empty() && !waiting.empty()) {
+    // requests that wait for one another while others keep the device busy
+    // (light requests, which free little) are a deadlock too once it lasts
+    int longest = 0;
+    for (int i : waiting) longest = std::max(longest, sv.waited[i]);
+    const bool stuck = waiting.size() >= 2 && longest >= kServeWaitSteps;
+    if ((!progress || stuck) && fin.empty() && !waiting.empty()) {
       if (waiting.size() == 1) {
         const int i = waiting[0];
         InstDev& d = sv.H[i].d;
@@ -1612,6 +1638,7 @@ struct Engine {
         free_buffers(sv.H[v]);
         sv.H[v] = InstHost{};
         sv.busy[v] = 0;
+        for (int i : waiting) sv.waited[i] = 0;
         sv.queue.push_front(std::move(sv.req[v]));
         sv.queue.front().in.words = sv.queue.front().words.data();
         sv.queue.front().in.lengths = sv.queue.front().lengths.data();
