@@ -175,9 +175,14 @@ vfb_status vfb_solve_noalloc(const vfb_instance *inst, vfb_result *out);
  * free slots while the bytes the resident instances are projected to hold
  * after their next level (last level-over-level growth) stay under
  * budget_frac of the memory budget (the head of the queue is admitted
- * whenever no slot is busy), builds one more level of every resident
- * instance, and returns the finished ones (up to cap) with their tags;
- * results equal vfb_solve's.  An instance whose buffers would grow past
+ * whenever no slot is busy; past that, a light request is still admitted
+ * when its first buffers fit the budget beside what is live), builds one
+ * more level of every resident instance, and returns the finished ones (up
+ * to cap) with their tags; results equal vfb_solve's.  A growth that finds
+ * the memory held by other requests waits for it; requests that can only
+ * wait for one another (none can go on, or two or more have waited 32
+ * steps) give way: the least advanced one is evicted and queued again at
+ * the front, to start over.  An instance whose buffers would grow past
  * request_bytes finishes with VFB_LIMIT and the sizes it completed.
  * *active / *queued (may be NULL) report the slots in use and the requests
  * waiting.  A request that cannot be admitted finishes with its status.
