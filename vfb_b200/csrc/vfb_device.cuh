@@ -26,8 +26,9 @@ constexpr int kP1TileTarget = 4096;   // shrink the staged height until a level 
 constexpr int kTuneBands = 16;
 constexpr int kMaxProbes = 4096;      // bounded linear probing
 // first buffers of at most this many table + bitmap bytes are initialised by
-// k_init's CTA for the instance instead of by two memsets each
-constexpr uint64_t kInitFillMax = 4ull << 20;
+// one k_fill launch for every new instance of the call instead of by two
+// memsets each (larger ones keep their memsets)
+constexpr uint64_t kInitFillMax = 64ull << 20;
 constexpr uint64_t kEmpty = ~0ULL;
 constexpr int kPayShift = 58;         // payload = level << 58 | candidate index
 constexpr uint64_t kIdxMask = (1ULL << kPayShift) - 1;
@@ -132,7 +133,7 @@ struct InstDev {
   unsigned long long best_cand;  // min candidate index whose CS satisfies the sample (P1)
   unsigned long long best_sol;   // min candidate index of a solution owning its key
   int sol_known;                 // best_sol settled before the rows were emitted
-  int fill;                      // 1: the table and the bitmap are still to be initialised (k_init)
+  int fill;                      // 1: the table and the bitmap are still to be initialised (k_fill)
   unsigned long long n_newlist;  // slots of keys first inserted by this level's P1 (listed in wins)
   int attempt, attempt_level;    // attempts at the current level (> 1: a retry after growth)
   int planned, p1_tail;          // level the current plan (bases, tiling) was made for (0: none);

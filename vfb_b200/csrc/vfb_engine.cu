@@ -687,8 +687,8 @@ struct Engine {
     d.bitmap_words = g4 / 4;
     d.wins = (uint64_t*)pw;
     d.tent_cap = std::min(g5, g6) / 8;
-    // small buffers are initialised by k_init (which runs next), one CTA per
-    // instance, in place of two API calls each
+    // small buffers are initialised by k_fill (launched once for all new
+    // instances before k_init) in place of two API calls each
     const uint64_t fill_bytes = (d.table_mask + 1) * sizeof(Slot) + d.bitmap_words * 4;
     d.fill = fill_bytes <= kInitFillMax ? 1 : 0;
     if (!d.fill) {
@@ -1072,8 +1072,9 @@ struct Engine {
     }
     if (rc == VFB_OK) {
       if (profile) cudaEventRecord(ev_k[0], stream);
+      k_fill<<<grid, 256, 0, stream>>>(dB);
       k_init<<<std::min(n, grid), 256, 0, stream>>>(dB);
-      ++c_launch;
+      c_launch += 2;
       if (profile) {
         cudaEventRecord(ev_k[1], stream);
         cudaStreamSynchronize(stream);
@@ -1345,6 +1346,7 @@ struct Engine {
     vfb_instance in;
     std::vector<uint64_t> words;
     std::vector<int> lengths;
+    bool evicted = false;   // gave its slot up for memory: waits until no request waits
   };
   struct Session {
     int cap = 0;
@@ -1355,6 +1357,7 @@ struct Engine {
     std::vector<uint64_t> proj;   // projected bytes of each busy slot after its next level
     std::vector<Pending> req;     // the request each busy slot holds (requeued if it is evicted)
     std::vector<int> waited;      // consecutive steps each busy slot has waited for memory
+    bool pressure = false;        // some request waited for memory in the last step
     uint64_t evictions = 0;       // requests evicted and queued again (memory held by the others)
     InstDev* h_inst = nullptr;    // pinned mirror of the slot records
     int p1_smem = 0;
@@ -1491,6 +1494,9 @@ struct Engine {
       // its first buffers fit the memory budget beside what is live now
       const bool over = mem_limit && nbusy > 0 && (double)committed > budget;
       Pending& p = sv.queue.front();
+      // an evicted request comes back once no request waits for memory
+      // (else it would take memory the waiting ones need and be evicted again)
+      if (p.evicted && sv.pressure && nbusy > 0) break;
       InstHost& H = sv.H[i];
       H = InstHost{};
       vfb_status s = prepare(p.in, H);
@@ -1557,8 +1563,9 @@ struct Engine {
       admitted = true;
     }
     if (admitted) {
+      k_fill<<<grid, 256, 0, stream>>>(dB);
       k_init<<<std::min(sv.cap, grid), 256, 0, stream>>>(dB);
-      ++c_launch;
+      c_launch += 2;
     }
     // 2. one level for every active instance
     int running = 0;
@@ -1617,6 +1624,7 @@ struct Engine {
     }
     // requests that wait for one another while others keep the device busy
     // (light requests, which free little) are a deadlock too once it lasts
+    sv.pressure = !waiting.empty();
     int longest = 0;
     for (int i : waiting) longest = std::max(longest, sv.waited[i]);
     const bool stuck = waiting.size() >= 2 && longest >= kServeWaitSteps;
@@ -1639,6 +1647,7 @@ struct Engine {
         sv.H[v] = InstHost{};
         sv.busy[v] = 0;
         for (int i : waiting) sv.waited[i] = 0;
+        sv.req[v].evicted = true;
         sv.queue.push_front(std::move(sv.req[v]));
         sv.queue.front().in.words = sv.queue.front().words.data();
         sv.queue.front().in.lengths = sv.queue.front().lengths.data();

@@ -236,7 +236,10 @@ __device__ void plan_one(InstDev& I) {
   if (!on_the_fly) {   // an on-the-fly level stores nothing
     if (g > promote_above) need |= NEED_PROMOTE;
     if (words > bitmap_words) { need |= NEED_BITMAP; I.need_amount[0] = words; }
-    if (2 * (keys + est) > table_cap) { need |= NEED_TABLE; I.need_amount[1] = 4 * (keys + est); }
+    // (twice the projected keys, rounded up to a power of two: at most half
+    // full if the projection holds; 4x measured 6% slower on large
+    // instances, from filling and rehashing twice the bytes)
+    if (2 * (keys + est) > table_cap) { need |= NEED_TABLE; I.need_amount[1] = 2 * (keys + est); }
     if (lstart_k + est > row_cap) { need |= NEED_ROWS; I.need_amount[3] = lstart_k + est; }
     if (est > tent_cap) { need |= NEED_LIST; I.need_amount[2] = est; }
   }
@@ -1299,6 +1302,24 @@ __global__ void __launch_bounds__(kTS) k_cluster(ClusterWork W) {
   }
 }
 
+// ==================================================================== fill
+// First buffers of new instances (fill set by the host): empty table (every
+// word ~0) and clear owner bitmap, every thread of the grid on one instance
+// after the other.
+__global__ void k_fill(BatchDev* Bp) {
+  const BatchDev B = *Bp;
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+  for (int b = 0; b < B.ninst; ++b) {
+    const InstDev& I = B.inst[b];
+    if (!I.fill || I.status != ST_RUNNING || I.level != 1) continue;
+    ulonglong2* tab = reinterpret_cast<ulonglong2*>(I.table);
+    const uint64_t nt = (I.table_mask + 1) * (sizeof(Slot) / sizeof(ulonglong2));
+    for (uint64_t x = tid; x < nt; x += nth) tab[x] = make_ulonglong2(~0ULL, ~0ULL);
+    for (uint64_t x = tid; x < I.bitmap_words; x += nth) I.bitmap[x] = 0u;
+  }
+}
+
 // ==================================================================== init
 // Level 1: every proposition is a row (duplicates included); its key enters
 // the set; propositions are tested as size-1 solutions in order
@@ -1310,13 +1331,6 @@ __global__ void k_init(BatchDev* Bp) {
   for (int b = blockIdx.x; b < B.ninst; b += gridDim.x) {
     InstDev& I = B.inst[b];
     if (I.status != ST_RUNNING || I.level != 1) continue;
-    if (I.fill) {
-      // empty table (every word ~0) and clear owner bitmap
-      ulonglong2* tab = reinterpret_cast<ulonglong2*>(I.table);
-      const uint64_t nt = (I.table_mask + 1) * (sizeof(Slot) / sizeof(ulonglong2));
-      for (uint64_t x = threadIdx.x; x < nt; x += blockDim.x) tab[x] = make_ulonglong2(~0ULL, ~0ULL);
-      for (uint64_t x = threadIdx.x; x < I.bitmap_words; x += blockDim.x) I.bitmap[x] = 0u;
-    }
     if (threadIdx.x == 0) { s_first = ~0ULL; s_new = 0; }
     __syncthreads();
     for (int v = threadIdx.x; v < I.A; v += blockDim.x) {

@@ -147,6 +147,7 @@ __global__ void k_bs_bounds(BsDev D, unsigned long long nent, const unsigned lon
 __global__ void k_bs_leaves(const InstDev* I, const unsigned long long* rows, int n, int16_t* rpn, int* len);
 
 // Set-up and maintenance kernels.
+__global__ void k_fill(BatchDev* B);
 __global__ void k_init(BatchDev* B);
 __global__ void k_rehash(const Slot* old_tab, unsigned long long old_cap, Slot* new_tab,
                          unsigned long long new_mask, unsigned long long* fail);
