@@ -429,11 +429,29 @@ typedef struct {
     uint64_t l0, ln, r0, rn;
 } block_t;
 
+/* Blocks and batches of fewer chunks (of 4096 candidates) than this run on
+ * the calling thread. */
+#define ORC_PAR_MIN_CHUNKS 8
+
 static int run_block_parallel(search_t *s, const block_t *bk) {
     const orc_problem *p = s->p;
     const int T = s->T;
     const uint64_t n = op_is_unary(bk->op) ? bk->ln : bk->ln * bk->rn;
     const uint64_t BATCH = 1ULL << 20, CH = 4096;
+    if (n < (uint64_t)ORC_PAR_MIN_CHUNKS * CH) {
+        /* a small block on the calling thread, candidate by candidate: the
+         * team, the candidate lists and the in-order commit cost more than
+         * its candidates */
+        for (uint64_t a = 0; a < bk->ln; ++a) {
+            if (op_is_unary(bk->op)) {
+                if (process(s, bk->op, (int64_t)(bk->l0 + a), -1)) return 1;
+                continue;
+            }
+            for (uint64_t b = 0; b < bk->rn; ++b)
+                if (process(s, bk->op, (int64_t)(bk->l0 + a), (int64_t)(bk->r0 + b))) return 1;
+        }
+        return 0;
+    }
     int nthreads = p->threads > 1 ? p->threads : 1;
     pend_t **lists = (pend_t **)calloc((BATCH + CH - 1) / CH, sizeof(pend_t *));
     uint32_t *lcount = (uint32_t *)calloc((BATCH + CH - 1) / CH, sizeof(uint32_t));
@@ -441,7 +459,9 @@ static int run_block_parallel(search_t *s, const block_t *bk) {
     for (uint64_t base = 0; base < n && !stop; base += BATCH) {
         const uint64_t cnt = (n - base) < BATCH ? (n - base) : BATCH;
         const int64_t nch = (int64_t)((cnt + CH - 1) / CH);
-#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+        /* a batch of few chunks runs on the calling thread: starting the
+         * team costs more than its candidates */
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads) if (nch >= ORC_PAR_MIN_CHUNKS)
         for (int64_t c = 0; c < nch; ++c) {
             uint64_t cs[ORC_MAX_TRACES];
             const uint64_t t0 = base + (uint64_t)c * CH;
