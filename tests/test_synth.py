@@ -22,3 +22,21 @@ def test_configs_are_stable():
     assert synth.rpn_to_infix(c2.planted, c2.names) == "X((a2) | (~(X((G(a2)) U (a1)))))"
     batch = synth.config_batch(count=8)
     assert len(batch) == 8 and all(2 <= b.num_vars <= 8 for b in batch)
+
+
+def test_large_deep_seed_rule():
+    """The deep large instance is the first seed from 2 on whose large-shape
+    instance has no formula of size 9 or less: every seed before it is solved
+    by the oracle within size 9 (seed 2, the shape's own seed, by a single
+    proposition)."""
+    import os
+
+    import oracle
+    sizes = {}
+    for seed in range(2, synth.LARGE_DEEP_SEED):
+        inst = synth.config_large(seed, max_size=9)
+        r = oracle.solve(oracle.Problem.from_instance(inst, threads=os.cpu_count() or 1))
+        assert r["status"] == oracle.FOUND, (seed, r["status"])
+        sizes[seed] = r["size"]
+    assert sizes[2] == 1
+    assert max(sizes.values()) <= 9

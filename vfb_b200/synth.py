@@ -327,37 +327,57 @@ def config_small(seed: int = 0) -> Instance:
             return Instance(2, pos, neg, 10, ["a0", "a1"], None, 3, "small")
 
 
-def config_planted(seed: int = 1) -> Instance:
+def config_planted(seed: int = 1, native: bool = True) -> Instance:
     """Planted single instance: 4 APs, size-9 planted formula, 20+20 traces of length 16."""
     rng = Rng(seed)
-    return planted_instance(rng, 4, 9, 20, 20, 16, 0.5, 13, name="planted")
+    return planted_instance(rng, 4, 9, 20, 20, 16, 0.5, 13, name="planted", native=native)
+
+
+# Memory budget of the large single instance's search: the level cache plus
+# the hash set stop growing at 150 GB of device memory (the level that does not
+# fit is then tested without being stored).
+LARGE_MEM_BYTES = 150 * 10**9
+
+# The large shape at seed 2 is solved by one proposition (a7: a size-1 search
+# of 8 characteristic sets).  The search the shape is meant to exercise -- deep
+# levels up to the size or memory limit -- is measured on the first seed from 2
+# on whose instance has no formula of size 9 or less: seed 12 (seeds 2-11 are
+# solved at sizes 1-9 by the oracle; tests/test_synth.py checks this).
+LARGE_DEEP_SEED = 12
 
 
 def config_large(seed: int = 2, length: int = 64, planted_size: int = 13,
-                 max_size: int = 17) -> Instance:
+                 max_size: int = 17, native: bool = True) -> Instance:
     """Planted large instance: 8 APs, 31 pos + 32 neg traces of length 64, p=0.3."""
     rng = Rng(seed)
     return planted_instance(rng, 8, planted_size, 31, 32, length, 0.3,
-                            max_size, name="large")
+                            max_size, name="large", native=native)
 
 
-def batch_instance(rng: Rng, idx: int = 0) -> Instance:
+def config_large_deep(max_size: int = 17, native: bool = True) -> Instance:
+    """The large shape at LARGE_DEEP_SEED: the deep, memory-bounded search."""
+    inst = config_large(LARGE_DEEP_SEED, max_size=max_size, native=native)
+    inst.name = f"large-s{LARGE_DEEP_SEED}"
+    return inst
+
+
+def batch_instance(rng: Rng, idx: int = 0, native: bool = True) -> Instance:
     """One instance of the mixed batch: A~U{2..8}, T~U{4..63}, L~U{4..64} per trace."""
     a = rng.uniform_int(2, 8)
     t = rng.uniform_int(4, 63)
     n_pos = t // 2 if rng.below(2) == 0 else (t + 1) // 2
     size = rng.uniform_int(5, 11)
     return planted_instance(rng, a, size, n_pos, t - n_pos, (4, 64), 0.5, size + 4,
-                            name=f"batch{idx}")
+                            name=f"batch{idx}", native=native)
 
 
-def config_batch(seed: int = 3, count: int = 256) -> list[Instance]:
+def config_batch(seed: int = 3, count: int = 256, native: bool = True) -> list[Instance]:
     rng = Rng(seed)
-    return [batch_instance(rng, i) for i in range(count)]
+    return [batch_instance(rng, i, native=native) for i in range(count)]
 
 
 def config_serving(seed: int = 4, count: int = 2000, rate: float = 100.0,
-                   large_frac: float = 0.05, large_fn=None):
+                   large_frac: float = 0.05, large_fn=None, native: bool = True):
     """Poisson request stream: (arrival_time_s, Instance) pairs.
 
     95% of requests are drawn like the mixed batch, 5% like the large instance
@@ -371,8 +391,8 @@ def config_serving(seed: int = 4, count: int = 2000, rate: float = 100.0,
         t += -math.log(1.0 - u) / rate
         if rng.random() < large_frac:
             s = rng.next_u64()
-            inst = (large_fn or (lambda sd: config_large(sd)))(s)
+            inst = (large_fn or (lambda sd: config_large(sd, native=native)))(s)
         else:
-            inst = batch_instance(rng, i)
+            inst = batch_instance(rng, i, native=native)
         out.append((t, inst))
     return out
