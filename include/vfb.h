@@ -156,11 +156,14 @@ vfb_status vfb_solve_exhaustive(void *ctx, const vfb_instance *inst, vfb_result 
  * default stream, with every device buffer carved from one static array of
  * VFB_NOALLOC_SCRATCH_BYTES that the library's module holds on every GPU that
  * loads it, until the process exits.  Buffers do not grow: the array holds a
- * hash set of 2^19 slots (kept at most half full), a bitmap of 2^25 candidates
- * per size, 2^19 owner-list entries, and about 40 MiB of level cache
- * (for 40 traces, about 110000 characteristic sets); a search that needs more
- * stops with VFB_OOM and a message on stderr.  The first call on a device resolves the array's
- * address and should come before any stream capture.  All calls share the
+ * hash set of 2^19 slots, a bitmap of 2^25 candidates per size, 2^19
+ * owner-list entries and about 40 MiB of level cache, which holds
+ * 40 MiB / (8*TP + 8) characteristic sets (TP = traces rounded up to even:
+ * about 127,000 at 40 traces, 40,000 at 128); at most about 2^18 distinct
+ * sets in all (the hash set is planned at most half full); a search that needs
+ * more stops with VFB_OOM and a message on stderr.  The first call on a device
+ * resolves the array's address and should come before any stream capture;
+ * after a device reset the next call resolves it again.  All calls share the
  * array (each one clears what must start empty); calls that overlap on the
  * GPU race, so serialise them.  Results equal vfb_solve's for every instance
  * that fits; device_seconds is not measured (0). */

@@ -21,12 +21,15 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 NOCACHE = os.path.join(REF_DIR, "ltl_nocache")
 LTL_BS = os.path.join(REF_DIR, "ltl_bs")
-DEFAULT_SRC = "/root/reference"
+# The reference checkout: VFB_REFERENCE_SRC, else a directory named
+# "reference" beside this repository's root.
+DEFAULT_SRC = os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
 
 
 def build_if_present(src: str | None = None, force: bool = False) -> bool:
-    """Compile the reference programs if their sources are available."""
-    src = src or os.environ.get("VFB_REFERENCE_SRC", DEFAULT_SRC)
+    """Compile the reference programs from the sources in `src` (default:
+    VFB_REFERENCE_SRC, else DEFAULT_SRC) if they are there."""
+    src = src or os.environ.get("VFB_REFERENCE_SRC") or DEFAULT_SRC
     if not os.path.exists(os.path.join(src, "LTL_BS.cu")):
         return False
     os.makedirs(REF_DIR, exist_ok=True)

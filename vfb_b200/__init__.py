@@ -18,6 +18,7 @@ from __future__ import annotations
 import array
 import ctypes
 import os
+import threading
 from dataclasses import dataclass, field
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -424,13 +425,21 @@ class Engine:
         return [_result(res[i]) for i in range(n)]
 
 
+_noalloc_lock = threading.Lock()
+
+
 def solve_noalloc(prob: Problem) -> Result:
     """vfb_solve_noalloc: the solve without any allocation (static scratch of
-    VFB_NOALLOC_SCRATCH_BYTES on the current device; VFB_OOM if it does not fit)."""
+    VFB_NOALLOC_SCRATCH_BYTES on the current device; VFB_OOM if it does not fit).
+
+    Every call uses the same static device array, and the C call releases the
+    GIL, so calls from several Python threads would race on it: they are
+    serialised here by a module-level lock."""
     lib = load_library()
     inst, keep = prob._cstruct()
     res = _Result()
-    lib.vfb_solve_noalloc(ctypes.byref(inst), ctypes.byref(res))
+    with _noalloc_lock:
+        lib.vfb_solve_noalloc(ctypes.byref(inst), ctypes.byref(res))
     del keep
     return _result(res)
 

@@ -26,7 +26,17 @@
 // array; serialise them.  The first call on a device resolves the array's
 // device address (cudaGetSymbolAddress with that device current) and sets the
 // P1 kernel's shared-memory limit; make that first call before any stream
-// capture begins.
+// capture begins.  The address is remembered with the CUDA context it was
+// resolved in: after a device reset (a new primary context) the next call
+// resolves it again, so it never writes through an address of a context that
+// is gone.
+//
+// Capacity: besides the fixed parts (hash set of 2^19 slots, 16 MiB; bitmap
+// of 2^25 candidates, 4 MiB; owner list of 2^19 entries, 4 MiB), about 40 MiB
+// of level cache: rows = that space / (8 * TP + 8) bytes, TP = traces rounded
+// up to even (about 127,000 characteristic sets at 40 traces, 40,000 at 128),
+// and at most about 2^18 distinct keys (the hash set is planned at most half
+// full, counting the next level's projected keys).
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -46,28 +56,68 @@ __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
 unsigned char* g_base[kMaxDevices] = {};
+void* g_base_ctx[kMaxDevices] = {};   // context each address was resolved in
 std::mutex g_mu;
 
+// The driver's cuCtxGetCurrent, looked up through the runtime so that the
+// library does not link the driver library itself.  nullptr if unavailable.
+using CtxGetCurrentFn = int (*)(void**);
+CtxGetCurrentFn ctx_get_current() {
+  static const CtxGetCurrentFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return static_cast<CtxGetCurrentFn>(nullptr);
+    }
+    return reinterpret_cast<CtxGetCurrentFn>(p);
+  }();
+  return fn;
+}
+
+void* current_context() {
+  void* c = nullptr;
+  const CtxGetCurrentFn fn = ctx_get_current();
+  if (fn && fn(&c) != 0) c = nullptr;
+  return c;
+}
+
 // Device address of g_scratch for device `dev` (current).  The host-side
-// symbol is only a stand-in and must never be passed to a kernel.
+// symbol is only a stand-in and must never be passed to a kernel.  Resolved
+// on the first call on a device and again whenever the current context is not
+// the one it was resolved in (the device was reset since).
 vfb_status scratch_base(int dev, unsigned char** out) {
   std::lock_guard<std::mutex> lock(g_mu);
   if (dev < 0 || dev >= kMaxDevices) return VFB_DEVICE_ERROR;
-  if (!g_base[dev]) {
+  void* ctx = g_base[dev] ? current_context() : nullptr;
+  if (!g_base[dev] || ctx != g_base_ctx[dev]) {
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_scratch) != cudaSuccess || !p) {
       cudaGetLastError();
+      g_base[dev] = nullptr;
       return VFB_DEVICE_ERROR;
     }
     const int smem = (kTS * (kMaxTraces + 1) + kTQ * kMaxTraces) * 8;
     if (cudaFuncSetAttribute(k_p1, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) {
       cudaGetLastError();
+      g_base[dev] = nullptr;
       return VFB_DEVICE_ERROR;
     }
     g_base[dev] = static_cast<unsigned char*>(p);
+    g_base_ctx[dev] = current_context();   // (the lookup above made the context current)
   }
   *out = g_base[dev];
   return VFB_OK;
+}
+
+// Proposition rows from the caller's trace-major words (words[t*A + v] ->
+// rows[v*TP + t], zero in the padding column).
+__global__ void k_na_rows(const uint64_t* __restrict__ words, int T, int A, int TP, uint64_t* __restrict__ rows) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A * TP; i += gridDim.x * blockDim.x) {
+    const int v = i / TP, t = i - v * TP;
+    rows[i] = t < T ? words[(size_t)t * A + v] : 0ULL;
+  }
 }
 
 struct Carver {
@@ -190,6 +240,7 @@ extern "C" vfb_status vfb_solve_noalloc(const vfb_instance* inst, vfb_result* ou
   d.bitmap_words = kNaWords;
   d.wins = cv.take<uint64_t>(kNaTents);
   d.tent_cap = kNaTents;
+  uint64_t* stage = cv.take<uint64_t>((size_t)d.T * d.A);   // the caller's words, as given
   const size_t used = ((cv.off + 255) & ~size_t(255)) + 512;   // + alignment of the last two carves
   const size_t per_row = (size_t)d.TP * 8 + 8;                  // row words + origin index
   if (used >= kScratchBytes || (kScratchBytes - used) / per_row < (size_t)d.A) {
@@ -207,11 +258,13 @@ extern "C" vfb_status vfb_solve_noalloc(const vfb_instance* inst, vfb_result* ou
   cudaStream_t st = 0;
   bool ok = cudaMemsetAsync(d.table, 0xFF, kNaSlots * sizeof(Slot), st) == cudaSuccess &&
             cudaMemsetAsync(d.bitmap, 0, kNaWords * 4, st) == cudaSuccess;
-  uint64_t row[kMaxTraces];   // one proposition's row, staged on the stack
-  for (int v = 0; ok && v < d.A; ++v) {
-    for (int t = 0; t < d.TP; ++t) row[t] = t < d.T ? inst->words[(size_t)t * d.A + v] : 0ULL;
-    ok = cudaMemcpy(d.rows + (size_t)v * d.TP, row, (size_t)d.TP * 8, cudaMemcpyHostToDevice) == cudaSuccess;
-    h2d += (uint64_t)d.TP * 8;
+  // one copy of the words, turned into proposition rows on the device
+  ok = ok && cudaMemcpy(stage, inst->words, (size_t)d.T * d.A * 8, cudaMemcpyHostToDevice) == cudaSuccess;
+  h2d += (uint64_t)d.T * d.A * 8;
+  if (ok) {
+    k_na_rows<<<(d.A * d.TP + 255) / 256, 256, 0, st>>>(stage, d.T, d.A, d.TP, d.rows);
+    ++launches;
+    ok = cudaGetLastError() == cudaSuccess;
   }
   ok = ok && cudaMemcpy(dI, &d, sizeof(InstDev), cudaMemcpyHostToDevice) == cudaSuccess &&
        cudaMemcpy(dB, &hB, sizeof(BatchDev), cudaMemcpyHostToDevice) == cudaSuccess;
