@@ -21,6 +21,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 NOCACHE = os.path.join(REF_DIR, "ltl_nocache")
 LTL_BS = os.path.join(REF_DIR, "ltl_bs")
+LTL_BS_TIMED = os.path.join(REF_DIR, "ltl_bs_timed")   # built with -DMEASUREMENT_MODE
 # The reference checkout: VFB_REFERENCE_SRC, else a directory named
 # "reference" beside this repository's root.
 DEFAULT_SRC = os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
@@ -41,6 +42,12 @@ def build_if_present(src: str | None = None, force: bool = False) -> bool:
         jobs.append(["nvcc", os.path.join(src, "LTL_BS.cu"), "-I",
                      os.path.join(src, "modified_libraries"), "--extended-lambda", "-o", LTL_BS,
                      "-arch=sm_100a", "-std=c++20"])
+    if force or not os.path.exists(LTL_BS_TIMED):
+        # the same program with its timing output (Running Time, Cost of Final
+        # LTL; LTL_BS.cu:1661-1671, 1706-1710) in place of the progress lines
+        jobs.append(["nvcc", os.path.join(src, "LTL_BS.cu"), "-I",
+                     os.path.join(src, "modified_libraries"), "--extended-lambda", "-o", LTL_BS_TIMED,
+                     "-arch=sm_100a", "-std=c++20", "-DMEASUREMENT_MODE"])
     procs = [subprocess.Popen(j, stdout=subprocess.PIPE, stderr=subprocess.STDOUT) for j in jobs]
     ok = True
     for p in procs:
@@ -110,6 +117,26 @@ def run_ltl_bs(txt_path: str, max_size: int, rlx_type: int = 3, timeout: float =
     res = parse_ltl_bs(out.stdout)
     res["returncode"] = out.returncode
     return res
+
+
+def run_ltl_bs_timed(txt_path: str, max_size: int, rlx_type: int = 3, timeout: float = 300,
+                     env: dict | None = None) -> dict:
+    """One run of the timed LTL_BS build with unit costs and no BS stage:
+    its own Running Time (the LTLI call, LTL_BS.cu:1661-1671), the final
+    cost and the formula."""
+    args = [LTL_BS_TIMED, txt_path] + ["1"] * 8 + [str(max_size), str(max_size), str(rlx_type), "1"]
+    out = subprocess.run(args, capture_output=True, text=True, timeout=timeout, env=env)
+    t = re.search(r"Running Time:\s*([0-9.eE+-]+)\s*s", out.stdout)
+    c = re.search(r"Cost of Final LTL:\s*(-?\d+)", out.stdout)
+    n = re.search(r"Number of All LTLs:\s*(\d+)", out.stdout)
+    f = re.search(r'LTL: "(.*)"', out.stdout)
+    return {"returncode": out.returncode, "seconds": float(t.group(1)) if t else None,
+            "cost": int(c.group(1)) if c else None, "all_ltls": int(n.group(1)) if n else None,
+            "formula": f.group(1) if f else None}
+
+
+def timed_available() -> bool:
+    return os.path.exists(LTL_BS_TIMED)
 
 
 # ----------------------------------------------- formula text -> RPN tokens

@@ -50,6 +50,8 @@ enum Status : int {
 enum NeedBits : int {
   NEED_BITMAP = 1, NEED_TABLE = 2, NEED_LIST = 4, NEED_ROWS = 8, NEED_LIMIT = 16,
   NEED_PROMOTE = 32,   // level too large for the cluster solver: continue on the whole GPU
+  NEED_ROWS_EST = 64,  // with NEED_ROWS: the rows were asked for by the plan's projection (the
+                       // level's owners are not known yet), not by the owner count
 };
 
 enum KeyMode : int { KEY_CONCAT = 0, KEY_SAMPLED = 1, KEY_HASH = 3 };
@@ -122,7 +124,8 @@ struct InstDev {
   int p1_masked;   // a P1 tile of this attempt skipped operators past best_cand
   int no_mask;     // this level is re-run without skipping (set by the table scan)
   int mask_off;    // never skip (contexts that cannot re-run a level)
-  int pad_m;
+  int rows_deferred;  // the projected rows of this level did not fit the budget: the level
+                      // runs without them and the owner count after the table scan decides
   int ngroups;
   int tq;                      // staged rows per P1 tile at this level (1..kTQ)
   int p1_blocks;               // P1 CTAs this level asks for (0: every resident CTA)

@@ -774,30 +774,63 @@ struct Engine {
                    (unsigned long long)d.need_amount[0], (unsigned long long)d.need_amount[2]);
     if (need & NEED_LIMIT) return VFB_LIMIT;
     if (need & NEED_PROMOTE) d.promote_above = ~0ULL;   // continue on the whole GPU
+    // rows the plan projected (not yet the level's owner count): when they
+    // cannot be had, the level runs without them and its table scan asks for
+    // exactly what its owners need (nothing if it settles the solution)
+    const bool rows_est = (need & NEED_ROWS) && (need & NEED_ROWS_EST);
+    const uint64_t row_bytes = (uint64_t)d.TP * 8 + 8;
+    bool rows_wanted = (need & NEED_ROWS) != 0;
+    // bytes the rows may add under the per-request cap (no cap: unbounded)
+    uint64_t rows_room = ~0ULL;
     if (cap_bytes) {
       uint64_t add = 0;
-      if (need & NEED_ROWS)
-        add += std::max<uint64_t>(2 * d.row_cap, d.need_amount[3] + d.need_amount[3] / 4) * ((uint64_t)d.TP * 8 + 8);
       if (need & NEED_TABLE)
         add += pow2_at_least(std::max<uint64_t>(2 * (d.table_mask + 1), d.need_amount[1])) * sizeof(Slot);
       if (need & NEED_BITMAP) add += std::max<uint64_t>(2 * d.bitmap_words, d.need_amount[0] + d.need_amount[0] / 4) * 4;
       if (need & NEED_LIST) add += std::max<uint64_t>(2 * d.tent_cap, d.need_amount[2] + d.need_amount[2] / 4) * 8;
       if (inst_bytes(d) + add > cap_bytes) return VFB_LIMIT;
+      rows_room = cap_bytes - inst_bytes(d) - add;
+      if (rows_wanted && (d.need_amount[3] + d.need_amount[3] / 64 - std::min(d.need_amount[3], d.row_cap)) *
+                                 row_bytes > rows_room) {
+        if (!rows_est) return VFB_LIMIT;
+        rows_wanted = false;
+        d.rows_deferred = 1;
+        d.need &= ~(NEED_ROWS | NEED_ROWS_EST);
+      }
     }
-    if (need & NEED_ROWS) {
-      const uint64_t want = std::max<uint64_t>(2 * d.row_cap, d.need_amount[3] + d.need_amount[3] / 4);
+    if (rows_wanted) {
+      const uint64_t exact = d.need_amount[3];
       const uint64_t used = d.lstart[d.level];
-      void* pr = dalloc(want * (size_t)d.TP * 8, &g1);
-      void* po = pr ? dalloc(want * 8, &g2) : nullptr;
-      if (!pr || !po) { dfree(pr); return VFB_OOM; }
-      cudaMemcpyAsync(pr, d.rows, used * (size_t)d.TP * 8, cudaMemcpyDeviceToDevice, stream);
-      cudaMemcpyAsync(po, d.origin, used * 8, cudaMemcpyDeviceToDevice, stream);
-      dfree(d.rows);
-      dfree(d.origin);
-      d.rows = (uint64_t*)pr;
-      d.origin = (uint64_t*)po;
-      d.row_cap = std::min<uint64_t>(g1 / ((size_t)d.TP * 8), g2 / 8);
-      d.need &= ~NEED_ROWS;   // a later part that fails leaves this one done
+      // doubling keeps the number of growths small; when that does not fit
+      // (the budget or the per-request cap), the rows asked for and 1/64
+      // more are tried before giving up
+      const uint64_t tries[2] = {std::max<uint64_t>(2 * d.row_cap, exact + exact / 4), exact + exact / 64};
+      void* pr = nullptr;
+      void* po = nullptr;
+      for (int t = 0; t < 2 && !pr; ++t) {
+        const uint64_t want = tries[t];
+        if ((want - std::min(want, d.row_cap)) * row_bytes > rows_room) continue;
+        pr = dalloc(want * (size_t)d.TP * 8, &g1);
+        po = pr ? dalloc(want * 8, &g2) : nullptr;
+        if (!po) {
+          dfree(pr);
+          pr = nullptr;
+        }
+      }
+      if (!pr) {
+        if (!rows_est) return VFB_OOM;
+        d.rows_deferred = 1;
+        d.need &= ~(NEED_ROWS | NEED_ROWS_EST);
+      } else {
+        cudaMemcpyAsync(pr, d.rows, used * (size_t)d.TP * 8, cudaMemcpyDeviceToDevice, stream);
+        cudaMemcpyAsync(po, d.origin, used * 8, cudaMemcpyDeviceToDevice, stream);
+        dfree(d.rows);
+        dfree(d.origin);
+        d.rows = (uint64_t*)pr;
+        d.origin = (uint64_t*)po;
+        d.row_cap = std::min<uint64_t>(g1 / ((size_t)d.TP * 8), g2 / 8);
+        d.need &= ~(NEED_ROWS | NEED_ROWS_EST);   // a later part that fails leaves this one done
+      }
     }
     if (need & NEED_TABLE) {
       const uint64_t cap = d.table_mask + 1;

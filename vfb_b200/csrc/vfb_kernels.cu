@@ -60,7 +60,7 @@ __device__ void plan_one(InstDev& I) {
   const uint64_t lstart_prev = I.lstart[k - 1];
   const uint64_t keys = I.keys, table_cap = I.table_mask + 1, bitmap_words = I.bitmap_words,
                  row_cap = I.row_cap, tent_cap = I.tent_cap, promote_above = I.promote_above;
-  const int attempt = I.attempt, attempt_level = I.attempt_level;
+  const int attempt = I.attempt, attempt_level = I.attempt_level, rows_deferred = I.rows_deferred;
   const uint64_t lstart_k = lstart_prev + n[k - 1];
   I.lstart[k] = lstart_k;
   // candidate blocks in canonical order: ~ & | X F G U; a unary operator of
@@ -240,7 +240,12 @@ __device__ void plan_one(InstDev& I) {
     // full if the projection holds; 4x measured 6% slower on large
     // instances, from filling and rehashing twice the bytes)
     if (2 * (keys + est) > table_cap) { need |= NEED_TABLE; I.need_amount[1] = 2 * (keys + est); }
-    if (lstart_k + est > row_cap) { need |= NEED_ROWS; I.need_amount[3] = lstart_k + est; }
+    // (a projection the host cannot hold is deferred: the table scan asks for
+    // the rows the level's owners need, none when it settles the solution)
+    if (!rows_deferred && lstart_k + est > row_cap) {
+      need |= NEED_ROWS | NEED_ROWS_EST;
+      I.need_amount[3] = lstart_k + est;
+    }
     if (est > tent_cap) { need |= NEED_LIST; I.need_amount[2] = est; }
   }
   if (need) {
@@ -882,6 +887,7 @@ __device__ void finish_one(InstDev& I) {
     if (k >= max_size) I.status = ST_NOT_FOUND;
     else I.level = k + 1;
   }
+  I.rows_deferred = 0;   // the next level projects its rows afresh
 }
 
 __device__ void ph_finish(const BatchDev& B, unsigned bid, unsigned nb) {
