@@ -774,37 +774,44 @@ struct Engine {
                    (unsigned long long)d.need_amount[0], (unsigned long long)d.need_amount[2]);
     if (need & NEED_LIMIT) return VFB_LIMIT;
     if (need & NEED_PROMOTE) d.promote_above = ~0ULL;   // continue on the whole GPU
-    // rows the plan projected (not yet the level's owner count): when they
-    // cannot be had, the level runs without them and its table scan asks for
-    // exactly what its owners need (nothing if it settles the solution)
+    // Rows the plan projected (not yet the level's owner count) that the
+    // budget cannot hold next to the instance's other buffers are deferred:
+    // the level runs without them and its table scan asks for exactly what its
+    // owners need (nothing if it settles the solution).  The test depends on
+    // the instance alone (never on memory that other instances of a batch or
+    // a serving session hold: those wait), so batched and served results stay
+    // those of solo solves.
     const bool rows_est = (need & NEED_ROWS) && (need & NEED_ROWS_EST);
     const uint64_t row_bytes = (uint64_t)d.TP * 8 + 8;
     bool rows_wanted = (need & NEED_ROWS) != 0;
-    // bytes the rows may add under the per-request cap (no cap: unbounded)
-    uint64_t rows_room = ~0ULL;
-    if (cap_bytes) {
-      uint64_t add = 0;
-      if (need & NEED_TABLE)
-        add += pow2_at_least(std::max<uint64_t>(2 * (d.table_mask + 1), d.need_amount[1])) * sizeof(Slot);
-      if (need & NEED_BITMAP) add += std::max<uint64_t>(2 * d.bitmap_words, d.need_amount[0] + d.need_amount[0] / 4) * 4;
-      if (need & NEED_LIST) add += std::max<uint64_t>(2 * d.tent_cap, d.need_amount[2] + d.need_amount[2] / 4) * 8;
-      if (inst_bytes(d) + add > cap_bytes) return VFB_LIMIT;
-      rows_room = cap_bytes - inst_bytes(d) - add;
-      if (rows_wanted && (d.need_amount[3] + d.need_amount[3] / 64 - std::min(d.need_amount[3], d.row_cap)) *
-                                 row_bytes > rows_room) {
-        if (!rows_est) return VFB_LIMIT;
+    uint64_t add = 0;   // bytes the other buffers grow by
+    if (need & NEED_TABLE)
+      add += pow2_at_least(std::max<uint64_t>(2 * (d.table_mask + 1), d.need_amount[1])) * sizeof(Slot);
+    if (need & NEED_BITMAP) add += std::max<uint64_t>(2 * d.bitmap_words, d.need_amount[0] + d.need_amount[0] / 4) * 4;
+    if (need & NEED_LIST) add += std::max<uint64_t>(2 * d.tent_cap, d.need_amount[2] + d.need_amount[2] / 4) * 8;
+    const uint64_t non_rows = inst_bytes(d) - d.row_cap * row_bytes + add;
+    const uint64_t limit = cap_bytes ? std::min<uint64_t>(cap_bytes, mem_limit ? mem_limit : ~0ULL)
+                                     : (mem_limit ? mem_limit : ~0ULL);
+    if (cap_bytes && inst_bytes(d) + add > cap_bytes) return VFB_LIMIT;
+    const uint64_t rows_min = d.need_amount[3] + d.need_amount[3] / 64;   // the smallest allocation tried
+    if (rows_wanted && rows_min * row_bytes + non_rows > limit) {
+      if (!rows_est) {
+        if (cap_bytes && rows_min * row_bytes + non_rows > cap_bytes) return VFB_LIMIT;
+      } else {
         rows_wanted = false;
         d.rows_deferred = 1;
         d.need &= ~(NEED_ROWS | NEED_ROWS_EST);
       }
     }
+    // bytes the rows may add under the per-request cap (no cap: unbounded)
+    const uint64_t rows_room = cap_bytes ? cap_bytes - inst_bytes(d) - add : ~0ULL;
     if (rows_wanted) {
       const uint64_t exact = d.need_amount[3];
       const uint64_t used = d.lstart[d.level];
       // doubling keeps the number of growths small; when that does not fit
       // (the budget or the per-request cap), the rows asked for and 1/64
       // more are tried before giving up
-      const uint64_t tries[2] = {std::max<uint64_t>(2 * d.row_cap, exact + exact / 4), exact + exact / 64};
+      const uint64_t tries[2] = {std::max<uint64_t>(2 * d.row_cap, exact + exact / 4), rows_min};
       void* pr = nullptr;
       void* po = nullptr;
       for (int t = 0; t < 2 && !pr; ++t) {
@@ -817,11 +824,8 @@ struct Engine {
           pr = nullptr;
         }
       }
-      if (!pr) {
-        if (!rows_est) return VFB_OOM;
-        d.rows_deferred = 1;
-        d.need &= ~(NEED_ROWS | NEED_ROWS_EST);
-      } else {
+      if (!pr) return VFB_OOM;   // (held by other instances, or the pool is fragmented)
+      {
         cudaMemcpyAsync(pr, d.rows, used * (size_t)d.TP * 8, cudaMemcpyDeviceToDevice, stream);
         cudaMemcpyAsync(po, d.origin, used * 8, cudaMemcpyDeviceToDevice, stream);
         dfree(d.rows);
