@@ -232,7 +232,7 @@ void vfb_profile_reset(void *ctx);
  * tiles_log2 12, every resident CTA).  Results never depend on the shape. */
 #define VFB_TUNE_BANDS 16
 typedef struct {
-  uint8_t rows[VFB_TUNE_BANDS];         /* staged rows per tile: 1, 2, 4, .. 32 */
+  uint8_t rows[VFB_TUNE_BANDS];         /* staged rows per tile: 1, 2, 4, .. 32 (above 16 acts as 16) */
   uint8_t tiles_log2[VFB_TUNE_BANDS];   /* tile count to reach by shorter tiles, log2 (1..40) */
   uint16_t blocks[VFB_TUNE_BANDS];      /* CTAs of the level's launch */
   float ms[VFB_TUNE_BANDS];             /* vfb_autotune: k_p1 time of the chosen shape summed
@@ -247,7 +247,7 @@ vfb_status vfb_tune_set(void *ctx, const vfb_tune *tune);
 vfb_status vfb_tune_get(void *ctx, vfb_tune *tune);
 
 /* Autotuner: solves the n sample instances once per candidate shape (staged
- * rows 4/8/16/32 x tile targets 2^8/2^10/2^12/2^14 x every resident CTA or one
+ * rows 2/4/8/16 x tile targets 2^8/2^10/2^12/2^14 x every resident CTA or one
  * per SM), `reps` times each (>= 1), timing k_p1 at every level with CUDA events;
  * each band takes the shape with the least time over the sample's levels in
  * that band (bands without a level keep the built-in shape).  The result is

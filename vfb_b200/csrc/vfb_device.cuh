@@ -18,7 +18,11 @@ constexpr int kMaxSplits = 16;        // floor((32-1)/2)
 // binary level pairs; with unit costs, 1 + floor((k-1)/2)
 constexpr int kGroups = 64;
 constexpr int kTS = 128;              // stream rows per P1 tile (= threads per CTA)
-constexpr int kTQ = 32;               // staged rows per P1 tile (maximum)
+// Staged rows per P1 tile (maximum).  The shared memory of a tile holds kTS
+// stream rows and kTQ staged rows; 16 rather than 32 lets three CTAs share an
+// SM at 64 words per row instead of two (k_p1 of the large instance 40 ->
+// 34 ms), and 32 staged rows gained under 1% where the autotuner chose them.
+constexpr int kTQ = 16;
 constexpr int kTQDefault = 16;        // staged rows per P1 tile unless the tune table says otherwise
 constexpr int kP1TileTarget = 4096;   // shrink the staged height until a level has this many tiles
 // P1 launch shape per level band (tuned by the host): band b holds the levels

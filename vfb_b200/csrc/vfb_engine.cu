@@ -2142,7 +2142,7 @@ struct Engine {
     }
     for (int b = 0; b < kTuneBands; ++b) {
       const int r = t->rows[b];
-      if (r > kTQ || (r & (r - 1)) != 0) return VFB_BAD_INPUT;
+      if (r > 32 || (r & (r - 1)) != 0) return VFB_BAD_INPUT;   // (above kTQ acts as kTQ)
       if (t->tiles_log2[b] > 40) return VFB_BAD_INPUT;
     }
     tune = *t;
@@ -2166,7 +2166,7 @@ struct Engine {
     if (!sample || n <= 0 || reps < 1) return VFB_BAD_INPUT;
     struct Shape { uint8_t rows, tiles; uint16_t blocks; };
     std::vector<Shape> shapes;
-    for (int r : {4, 8, 16, 32})
+    for (int r : {2, 4, 8, 16})
       for (int t : {8, 10, 12, 14})
         for (int b : {0, sms}) shapes.push_back(Shape{(uint8_t)r, (uint8_t)t, (uint16_t)b});
     const int sv_profile = profile;
