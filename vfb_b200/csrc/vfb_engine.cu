@@ -97,6 +97,9 @@ struct Engine {
   // programmatic dependent launch between the kernels of a step (VFB_PDL=1):
   // measured 1-4% slower than plain stream order on every workload here
   bool use_pdl = false;
+  // P1 tiles staged by one bulk copy per operand block (VFB_P1_STAGING=bulk)
+  // instead of 8-byte asynchronous copies
+  bool p1_bulk = false;
   bool single_step = false;  // serving: one level per launch (admission between levels)
   bool use_coop = false;  // whole-GPU persistent cooperative solver (k_solve)
   int coop_grid = 0;
@@ -323,6 +326,10 @@ struct Engine {
     if (cudaFuncGetAttributes(&fa, k_p1) != cudaSuccess) return VFB_DEVICE_ERROR;
     if (cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsmem) != cudaSuccess)
       return VFB_DEVICE_ERROR;
+    if (cudaFuncSetAttribute(k_p1_bulk, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsmem) != cudaSuccess)
+      return VFB_DEVICE_ERROR;
+    const char* stg = std::getenv("VFB_P1_STAGING");
+    p1_bulk = stg && std::strcmp(stg, "bulk") == 0;
     const char* pdl_env = std::getenv("VFB_PDL");
     use_pdl = pdl_env && pdl_env[0] == '1';
     const char* env = std::getenv("VFB_NO_DEVICE_LOOP");
@@ -428,7 +435,7 @@ struct Engine {
       step_launch(false, k_advance, 1u, (unsigned)adv_threads, 0, dB, handle, built0, lp, mx);
       mark();
     }
-    step_launch(pdl && pre, k_p1, (unsigned)p1_grid, (unsigned)kTS, (size_t)p1_smem, dB);
+    step_launch(pdl && pre, p1_bulk ? k_p1_bulk : k_p1, (unsigned)p1_grid, (unsigned)kTS, (size_t)p1_smem, dB);
     mark();
     step_launch(pdl, k_table_scan_check, (unsigned)grid, 256u, 0, dB);
     mark();

@@ -310,10 +310,50 @@ __global__ void __launch_bounds__(1024) k_plan(BatchDev* Bp) {
 }
 
 // ======================================================================= P1
+// Bulk staging (BULK): a tile's stream rows and staged rows are each one
+// contiguous block of the level cache, copied into shared memory by one
+// cp.async.bulk apiece (issued by thread 0, completion counted by an
+// mbarrier in bytes).  The wait is bounded: a copy that has not landed after
+// about a second stops the instance with an error instead of hanging.
+constexpr long long kBulkWaitCycles = 2000000000LL;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+               ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
+}
+
+// true when the barrier's phase `parity` completed within the bound
+__device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t parity) {
+  const long long t0 = clock64();
+  for (;;) {
+    uint32_t done = 0;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                 " selp.u32 %0, 1, 0, p;\n}\n" : "=r"(done) : "r"(smem_addr(bar)), "r"(parity) : "memory");
+    if (done) return true;
+    if (clock64() - t0 > kBulkWaitCycles) return false;
+  }
+}
+
+template <bool BULK>
 __device__ void ph_p1(const BatchDev& B) {
   extern __shared__ __align__(16) uint64_t smem[];
   __shared__ TileSh P;
   __shared__ unsigned long long s_red[3][kTS / 32];
+  __shared__ __align__(8) uint64_t s_bar;
+  __shared__ int s_stop;
+  uint32_t phase = 0;
+  if (BULK) {
+    if (threadIdx.x == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(&s_bar)) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+      s_stop = 0;
+    }
+    __syncthreads();
+  }
   const unsigned long long total = B.p1_prefix[B.ninst];
   while (true) {
     if (threadIdx.x < 32) {
@@ -422,39 +462,57 @@ __device__ void ph_p1(const BatchDev& B) {
       P.off[t] = I.off[t];
       P.wid[t] = I.width[t];
     }
-    const int sp = P.TP + 1;                      // odd pitch: conflict-free row reads
+    // odd pitch for 8-byte copies (conflict-free row reads); the bulk copy
+    // keeps the rows' own pitch and rotates the word order instead
+    const int sp = BULK ? P.TP : P.TP + 1;
     uint64_t* sS = smem;
     uint64_t* sQ = smem + kTS * sp;
     P1Count cnt{0, 0, ~0ULL};
     // a tile whose every operator is skipped has nothing to do
-    const bool idle = P.skip || (!P.otf && P.mask == 0);
+    bool idle = P.skip || (!P.otf && P.mask == 0);
     if (!idle) {
       const int ns = (int)((P.nS - P.s0) < (uint64_t)kTS ? (P.nS - P.s0) : (uint64_t)kTS);
-      stage_rows(sS, sp, row_ptr(I, P.si, P.s0), ns, P.TP);
-      if (P.kind == 1) {
-        const int nq = (int)((P.nQ - P.q0) < (uint64_t)P.tq ? (P.nQ - P.q0) : (uint64_t)P.tq);
-        stage_rows(sQ, P.TP, row_ptr(I, P.qi, P.q0), nq, P.TP);
+      const int nq = P.kind == 1 ? (int)((P.nQ - P.q0) < (uint64_t)P.tq ? (P.nQ - P.q0) : (uint64_t)P.tq) : 0;
+      if (BULK) {
+        if (threadIdx.x == 0) {
+          // the previous tile's reads (generic proxy) come before these writes
+          asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+          const uint32_t bs = (uint32_t)ns * P.TP * 8, bq = (uint32_t)nq * P.TP * 8;
+          asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n"
+                       ::"r"(smem_addr(&s_bar)), "r"(bs + bq) : "memory");
+          bulk_copy(sS, row_ptr(I, P.si, P.s0), bs, &s_bar);
+          if (nq) bulk_copy(sQ, row_ptr(I, P.qi, P.q0), bq, &s_bar);
+        }
+        if (!bar_wait(&s_bar, phase)) {
+          *(volatile int*)&I.status = ST_ERROR;
+          s_stop = 1;
+        }
+        phase ^= 1u;
+      } else {
+        stage_rows(sS, sp, row_ptr(I, P.si, P.s0), ns, P.TP);
+        if (nq) stage_rows(sQ, P.TP, row_ptr(I, P.qi, P.q0), nq, P.TP);
+        stage_wait();
       }
-      stage_wait();
     }
     __syncthreads();
+    if (BULK && s_stop) break;
     if (!idle && P.otf) {
-      p1_solutions(I, P, sS, sp, sQ, cnt);
+      p1_solutions<BULK>(I, P, sS, sp, sQ, cnt);
     } else if (!idle) {
       // binary tiles compute the operators up to the last one kept (& | laUlb lbUla)
       const int keys = (P.mask & 8) ? 15 : (P.mask & 4) ? 7 : 3;
       switch (P.mode) {
         case KEY_HASH:
-          if (P.kind == 0) p1_unary<KEY_HASH>(I, P, sS, sp, cnt);
-          else p1_binary_keys<KEY_HASH>(keys, I, P, sS, sp, sQ, cnt);
+          if (P.kind == 0) p1_unary<KEY_HASH, BULK>(I, P, sS, sp, cnt);
+          else p1_binary_keys<KEY_HASH, BULK>(keys, I, P, sS, sp, sQ, cnt);
           break;
         case KEY_SAMPLED:
-          if (P.kind == 0) p1_unary<KEY_SAMPLED>(I, P, sS, sp, cnt);
-          else p1_binary_keys<KEY_SAMPLED>(keys, I, P, sS, sp, sQ, cnt);
+          if (P.kind == 0) p1_unary<KEY_SAMPLED, BULK>(I, P, sS, sp, cnt);
+          else p1_binary_keys<KEY_SAMPLED, BULK>(keys, I, P, sS, sp, sQ, cnt);
           break;
         default:
-          if (P.kind == 0) p1_unary<KEY_CONCAT>(I, P, sS, sp, cnt);
-          else p1_binary_keys<KEY_CONCAT>(keys, I, P, sS, sp, sQ, cnt);
+          if (P.kind == 0) p1_unary<KEY_CONCAT, BULK>(I, P, sS, sp, cnt);
+          else p1_binary_keys<KEY_CONCAT, BULK>(keys, I, P, sS, sp, sQ, cnt);
       }
     }
     // per-tile counter flush: warp reductions, then one atomic per counter
@@ -494,7 +552,18 @@ __global__ void __launch_bounds__(kTS) k_p1(BatchDev* Bp) {
   if (blockIdx.x >= B.p1_prefix[B.ninst]) return;   // more CTAs than tiles: no ticket needed
   const unsigned long long cap = B.tickets[kTicketP1Blocks];
   if (cap && blockIdx.x >= cap) return;               // the tuned CTA count of this step
-  ph_p1(B);
+  ph_p1<false>(B);
+}
+
+// k_p1 with bulk-copied tiles (VFB_P1_STAGING=bulk; measured against the
+// 8-byte copies of k_p1, see the design notes)
+__global__ void __launch_bounds__(kTS) k_p1_bulk(BatchDev* Bp) {
+  step_entry();
+  const BatchDev B = *Bp;
+  if (blockIdx.x >= B.p1_prefix[B.ninst]) return;
+  const unsigned long long cap = B.tickets[kTicketP1Blocks];
+  if (cap && blockIdx.x >= cap) return;
+  ph_p1<true>(B);
 }
 
 // ============================================================== table scan
@@ -1227,7 +1296,7 @@ __global__ void __launch_bounds__(kTS) k_solve(BatchDev* Bp, unsigned int max_st
     if (!grid_sync(ctl, nb)) return;
     if (bid == 0 && threadIdx.x == 0) ph_plan_prefix(B);
     if (!grid_sync(ctl, nb)) return;
-    ph_p1(B);
+    ph_p1<false>(B);
     if (!grid_sync(ctl, nb)) return;
     ph_table_scan(B, bid, nb);
     if (!grid_sync(ctl, nb)) return;
@@ -1290,7 +1359,7 @@ __global__ void __launch_bounds__(kTS) k_cluster(ClusterWork W) {
       cl.sync();
       if (rank == 0 && threadIdx.x == 0) ph_plan_prefix(B);
       cl.sync();
-      ph_p1(B);
+      ph_p1<false>(B);
       cl.sync();
       ph_table_scan(B, rank, csize);
       cl.sync();

@@ -59,6 +59,9 @@ __global__ void k_emit(BatchDev* B);
 // launched in this order for every level.
 __global__ void k_plan(BatchDev* B);
 __global__ void k_p1(BatchDev* B);
+// k_p1 with each tile's operand blocks staged by cp.async.bulk (an option:
+// VFB_P1_STAGING=bulk).
+__global__ void k_p1_bulk(BatchDev* B);
 __global__ void k_table_scan(BatchDev* B);
 __global__ void k_chunk_count(BatchDev* B);
 __global__ void k_chunk_scan(BatchDev* B);

@@ -408,6 +408,12 @@ __device__ __forceinline__ uint64_t pos_bit(const TileSh& P, int t) {
 template <bool HI>
 struct Half {
   static constexpr bool hi = HI;
+  static constexpr bool fixed = true;
+};
+// The half decided at run time (rotated word order of the bulk-staged tiles).
+struct HalfRt {
+  bool hi;
+  static constexpr bool fixed = false;
 };
 
 template <int MODE, bool HI>
@@ -420,11 +426,47 @@ __device__ __forceinline__ void key_word_h(KeyAcc& k, uint64_t w, int t, int off
   }
 }
 
+template <int MODE, typename H>
+__device__ __forceinline__ void key_word_any(KeyAcc& k, uint64_t w, int t, H half, int off, int width, int stride,
+                                             int L) {
+  if constexpr (H::fixed) {
+    key_word_h<MODE, H::hi>(k, w, t, off, width, stride, L);
+  } else if (MODE == KEY_HASH) {
+    const uint64_t x = splitmix_fin(w), m = half.hi ? ~0ULL : 0ULL;
+    k.a1 ^= x & m;
+    k.a0 ^= x & ~m;
+  } else {
+    key_word<MODE>(k, w, t, 0, off, width, stride, L);
+  }
+}
+
+// The trace words of a tile row in the order a thread visits them.  Copied
+// rows (odd pitch): 0..T-1, the words below T/2 first (the hash folds the two
+// halves into different words, chosen at compile time).  Bulk-staged rows
+// (pitch TP, even): lane l starts at word l mod T and wraps, so the 16 lanes
+// of a shared-memory wavefront read 16 different banks; the half is then
+// decided per word.
+template <bool BULK, typename F>
+__device__ __forceinline__ void p1_words(const TileSh& P, F&& body) {
+  if (!BULK) {
+    for (int t = 0; t < P.half; ++t) body(t, Half<true>{});
+    for (int t = P.half; t < P.T; ++t) body(t, Half<false>{});
+  } else {
+    int t = (threadIdx.x & 31) % P.T;
+    for (int i = 0; i < P.T; ++i) {
+      body(t, HalfRt{t < P.half});
+      if (++t == P.T) t = 0;
+    }
+  }
+}
+
 // Solution test accumulators: only bit 0 (step 0) of a word is compared
 // with the trace's label, so 32 bits carry the whole test.
 __device__ __forceinline__ uint32_t lo32(uint64_t w) { return (uint32_t)w; }
 
-template <int MODE>
+// BULK: rows staged by one bulk copy at the even pitch TP (rotated word
+// order), else by 8-byte copies at the odd pitch TP + 1.
+template <int MODE, bool BULK>
 __device__ inline void p1_unary(InstDev& I, const TileSh& P, const uint64_t* sS, int sp, P1Count& cnt) {
   const uint64_t a = P.s0 + threadIdx.x;
   const unsigned live = __ballot_sync(0xffffffffu, a < P.nS);
@@ -434,7 +476,6 @@ __device__ inline void p1_unary(InstDev& I, const TileSh& P, const uint64_t* sS,
   key_init(k0); key_init(k1); key_init(k2); key_init(k3);
   uint32_t bad[4] = {0, 0, 0, 0};
   auto body = [&](int t, auto half) {
-    constexpr bool HI = decltype(half)::hi;
     const uint64_t w = srow[t];
     const int L = P.len[t], off = P.off[t], wd = P.wid[t];
     const uint64_t lm = len_mask(L);
@@ -444,13 +485,12 @@ __device__ inline void p1_unary(InstDev& I, const TileSh& P, const uint64_t* sS,
     bad[1] |= lo32(w1) ^ pb;
     bad[2] |= lo32(w2) ^ pb;
     bad[3] |= lo32(w3) ^ pb;
-    key_word_h<MODE, HI>(k0, w0, t, off, wd, P.stride, L);
-    key_word_h<MODE, HI>(k1, w1, t, off, wd, P.stride, L);
-    key_word_h<MODE, HI>(k2, w2, t, off, wd, P.stride, L);
-    key_word_h<MODE, HI>(k3, w3, t, off, wd, P.stride, L);
+    key_word_any<MODE>(k0, w0, t, half, off, wd, P.stride, L);
+    key_word_any<MODE>(k1, w1, t, half, off, wd, P.stride, L);
+    key_word_any<MODE>(k2, w2, t, half, off, wd, P.stride, L);
+    key_word_any<MODE>(k3, w3, t, half, off, wd, P.stride, L);
   };
-  for (int t = 0; t < P.half; ++t) body(t, Half<true>{});
-  for (int t = P.half; t < P.T; ++t) body(t, Half<false>{});
+  p1_words<BULK>(P, body);
   uint64_t h[4], l[4], g[4];
   key_final<MODE>(k0, h[0], l[0]);
   key_final<MODE>(k1, h[1], l[1]);
@@ -467,7 +507,7 @@ __device__ inline void p1_unary(InstDev& I, const TileSh& P, const uint64_t* sS,
 
 // KEYS: the operators computed, a prefix of (&, |, laUlb, lbUla) as bits
 // 3, 7, 15; the inserted ones are P.mask within it.
-template <int MODE, int KEYS>
+template <int MODE, int KEYS, bool BULK>
 __device__ inline void p1_binary(InstDev& I, const TileSh& P, const uint64_t* sS, int sp, const uint64_t* sQ,
                           P1Count& cnt) {
   constexpr bool kO = (KEYS & 2) != 0, kU = (KEYS & 4) != 0, kV = (KEYS & 8) != 0;
@@ -486,32 +526,30 @@ __device__ inline void p1_binary(InstDev& I, const TileSh& P, const uint64_t* sS
     if (kV) key_init(kVn);
     uint32_t bad[4] = {0, 0, 0, 0};
     auto body = [&](int t, auto half) {
-      constexpr bool HI = decltype(half)::hi;
       const uint64_t qw = qrow[t], sw = srow[t];
       const uint64_t la = P.qleft ? qw : sw, lb = P.qleft ? sw : qw;
       const int L = P.len[t], off = P.off[t], wd = P.wid[t];
       const uint32_t pb = (uint32_t)pos_bit(P, t);
       const uint64_t wa = la & lb;
       bad[0] |= lo32(wa) ^ pb;
-      key_word_h<MODE, HI>(kA, wa, t, off, wd, P.stride, L);
+      key_word_any<MODE>(kA, wa, t, half, off, wd, P.stride, L);
       if (kO) {
         const uint64_t wo = la | lb;
         bad[1] |= lo32(wo) ^ pb;
-        key_word_h<MODE, HI>(kOr, wo, t, off, wd, P.stride, L);
+        key_word_any<MODE>(kOr, wo, t, half, off, wd, P.stride, L);
       }
       if (kU) {
         const uint64_t wu = w_until(la, lb);
         bad[2] |= lo32(wu) ^ pb;
-        key_word_h<MODE, HI>(kUn, wu, t, off, wd, P.stride, L);
+        key_word_any<MODE>(kUn, wu, t, half, off, wd, P.stride, L);
       }
       if (kV) {
         const uint64_t wv = w_until(lb, la);
         bad[3] |= lo32(wv) ^ pb;
-        key_word_h<MODE, HI>(kVn, wv, t, off, wd, P.stride, L);
+        key_word_any<MODE>(kVn, wv, t, half, off, wd, P.stride, L);
       }
     };
-    for (int t = 0; t < P.half; ++t) body(t, Half<true>{});
-    for (int t = P.half; t < P.T; ++t) body(t, Half<false>{});
+    p1_words<BULK>(P, body);
     const uint64_t a = P.qleft ? P.q0 + q : s;     // index in level i
     const uint64_t b = P.qleft ? s : P.q0 + q;     // index in level j
     const uint64_t ab = a * P.nj + b;
@@ -527,20 +565,21 @@ __device__ inline void p1_binary(InstDev& I, const TileSh& P, const uint64_t* sS
   }
 }
 
-template <int MODE>
+template <int MODE, bool BULK>
 __device__ inline void p1_binary_keys(int keys, InstDev& I, const TileSh& P, const uint64_t* sS, int sp,
                                       const uint64_t* sQ, P1Count& cnt) {
   switch (keys) {
-    case 15: p1_binary<MODE, 15>(I, P, sS, sp, sQ, cnt); break;
-    case 7: p1_binary<MODE, 7>(I, P, sS, sp, sQ, cnt); break;
+    case 15: p1_binary<MODE, 15, BULK>(I, P, sS, sp, sQ, cnt); break;
+    case 7: p1_binary<MODE, 7, BULK>(I, P, sS, sp, sQ, cnt); break;
     // & alone is computed with | (one variant less: a smaller kernel image
     // measured faster on small levels)
-    default: p1_binary<MODE, 3>(I, P, sS, sp, sQ, cnt);
+    default: p1_binary<MODE, 3, BULK>(I, P, sS, sp, sQ, cnt);
   }
 }
 
 // On-the-fly level (nothing stored): the tile's candidates get the solution
 // test alone, step 0 of every trace against its label; no key, no insert.
+template <bool BULK>
 __device__ inline void p1_solutions(InstDev& I, const TileSh& P, const uint64_t* sS, int sp, const uint64_t* sQ,
                                     P1Count& cnt) {
   const uint64_t s = P.s0 + threadIdx.x;
@@ -548,14 +587,14 @@ __device__ inline void p1_solutions(InstDev& I, const TileSh& P, const uint64_t*
   const uint64_t* srow = sS + threadIdx.x * sp;
   if (P.kind == 0) {
     uint32_t bad[4] = {0, 0, 0, 0};
-    for (int t = 0; t < P.T; ++t) {
+    p1_words<BULK>(P, [&](int t, auto) {
       const uint64_t w = srow[t], lm = len_mask(P.len[t]);
       const uint32_t pb = (uint32_t)pos_bit(P, t);
       bad[0] |= lo32(~w & lm) ^ pb;
       bad[1] |= lo32(w >> 1) ^ pb;
       bad[2] |= lo32(w_fin(w)) ^ pb;
       bad[3] |= lo32(w_glob(w, lm)) ^ pb;
-    }
+    });
     const uint64_t g[4] = {I.base_not + s, I.base_x + s, I.base_f + s, I.base_g + s};
 #pragma unroll
     for (int j = 0; j < 4; ++j)
@@ -566,7 +605,7 @@ __device__ inline void p1_solutions(InstDev& I, const TileSh& P, const uint64_t*
   for (int q = 0; q < nq; ++q) {
     const uint64_t* qrow = sQ + q * P.TP;
     uint32_t bad[4] = {0, 0, 0, 0};
-    for (int t = 0; t < P.T; ++t) {
+    p1_words<BULK>(P, [&](int t, auto) {
       const uint64_t qw = qrow[t], sw = srow[t];
       const uint64_t la = P.qleft ? qw : sw, lb = P.qleft ? sw : qw;
       const uint32_t pb = (uint32_t)pos_bit(P, t);
@@ -574,7 +613,7 @@ __device__ inline void p1_solutions(InstDev& I, const TileSh& P, const uint64_t*
       bad[1] |= lo32(la | lb) ^ pb;
       bad[2] |= lo32(w_until(la, lb)) ^ pb;
       bad[3] |= lo32(w_until(lb, la)) ^ pb;
-    }
+    });
     const uint64_t a = P.qleft ? P.q0 + q : s, b = P.qleft ? s : P.q0 + q;
     const uint64_t ab = a * P.nj + b;
     const uint64_t g[4] = {I.base_and[P.i] + ab, I.base_or[P.i] + ab, I.base_u[P.i] + ab, I.base_u[P.j] + b * P.ni + a};
