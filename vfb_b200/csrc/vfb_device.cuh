@@ -141,6 +141,8 @@ struct InstDev {
   unsigned long long best_sol;   // min candidate index of a solution owning its key
   int sol_known;                 // best_sol settled before the rows were emitted
   int fill;                      // 1: the table and the bitmap are still to be initialised (k_fill)
+  int atoms_staged;              // 1: the proposition rows wait in the batch's staging buffer at
+  uint64_t atom_off;             // word atom_off; k_init copies them into the level cache
   unsigned long long n_newlist;  // slots of keys first inserted by this level's P1 (listed in wins)
   int attempt, attempt_level;    // attempts at the current level (> 1: a retry after growth)
   int planned, p1_tail;          // level the current plan (bases, tiling) was made for (0: none);
@@ -153,7 +155,8 @@ struct InstDev {
   // figures of the last level built (for the host's profile): candidates,
   // owners, hash-set slots the owner scan visited, solution settled early
   unsigned long long built_cands, built_wins, built_scanned;
-  int built_sol_known, pad4;
+  int built_sol_known;
+  int emit_item;                 // owners per k_emit work item at this level (set by the table scan)
   // ---- result
   int res_size, rpn_len;
   int16_t rpn[kMaxSize];

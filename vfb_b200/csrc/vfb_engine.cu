@@ -123,6 +123,8 @@ struct Engine {
   unsigned long long* d_fail = nullptr;
   uint64_t* h_stage = nullptr;  // pinned upload staging
   size_t h_stage_words = 0;
+  uint64_t* d_atoms = nullptr;  // device staging of a batch's proposition rows (one upload)
+  size_t d_atoms_words = 0;
 
   // graphs
   cudaGraphExec_t exec = nullptr;
@@ -178,6 +180,9 @@ struct Engine {
     h_stage = nullptr;
     if (d_fail) cudaFree(d_fail);
     d_fail = nullptr;
+    if (d_atoms) cudaFree(d_atoms);
+    d_atoms = nullptr;
+    d_atoms_words = 0;
     if (h_ctl) cudaFreeHost(h_ctl);
     h_ctl = nullptr;
     if (d_slots) cudaFree(d_slots);
@@ -386,6 +391,7 @@ struct Engine {
       free_workspace();
       hB = nb;
       hB.chunk_cap = cc;
+      hB.atoms = d_atoms;   // (the staging buffer is not part of the workspace)
       dB = ndB;
       dInst = ndI;
       ninst_cap = nc;
@@ -961,7 +967,12 @@ struct Engine {
     return VFB_OK;
   }
 
-  vfb_status upload_atoms(const vfb_instance* ins, std::vector<InstHost>& H, int n) {
+  // Proposition rows of the instances with buffers (rows[v*TP + t] = words[t*A + v],
+  // zero padding).  staged: one copy of every instance's rows into the batch's
+  // staging buffer, which k_init copies into each level cache (a call of
+  // hundreds of instances makes one upload, not one per instance); else each
+  // instance's rows go to its level cache directly.
+  vfb_status upload_atoms(const vfb_instance* ins, std::vector<InstHost>& H, int n, bool staged = false) {
     size_t words = 0;
     for (int i = 0; i < n; ++i)
       if (H[i].active && H[i].d.rows) words += (size_t)H[i].d.A * H[i].d.TP;
@@ -982,11 +993,30 @@ struct Engine {
         if (d.TP > d.T) dst[(size_t)v * d.TP + d.T] = 0;
       }
       const size_t nb = (size_t)d.A * d.TP * 8;
-      if (cudaMemcpyAsync(d.rows, dst, nb, cudaMemcpyHostToDevice, stream) != cudaSuccess)
-        return dev_fail(__LINE__);
-      c_h2d += nb;
+      if (staged) {
+        H[i].d.atoms_staged = 1;
+        H[i].d.atom_off = o;
+      } else {
+        if (cudaMemcpyAsync(d.rows, dst, nb, cudaMemcpyHostToDevice, stream) != cudaSuccess)
+          return dev_fail(__LINE__);
+        c_h2d += nb;
+      }
       o += (size_t)d.A * d.TP;
     }
+    if (staged && o) {
+      if (o > d_atoms_words) {
+        if (cudaStreamSynchronize(stream) != cudaSuccess) return dev_fail(__LINE__);
+        if (d_atoms) cudaFree(d_atoms);
+        d_atoms = nullptr;
+        d_atoms_words = 0;
+        if (cudaMalloc(&d_atoms, o * 8) != cudaSuccess) return VFB_OOM;
+        d_atoms_words = o;
+      }
+      if (cudaMemcpyAsync(d_atoms, h_stage, o * 8, cudaMemcpyHostToDevice, stream) != cudaSuccess)
+        return dev_fail(__LINE__);
+      c_h2d += o * 8;
+    }
+    hB.atoms = d_atoms;
     return VFB_OK;
   }
 
@@ -1103,7 +1133,7 @@ struct Engine {
       H[i].active = true;
       chunk_need += (H[i].d.bitmap_words + kCompactWords - 1) / kCompactWords;
     }
-    rc = upload_atoms(ins, H, n);
+    rc = upload_atoms(ins, H, n, true);
     if (rc == VFB_OK) rc = ensure_workspace(n, chunk_need + n);
     if (rc == VFB_OK) {
       std::vector<InstDev> recs(n);

@@ -658,7 +658,7 @@ __global__ void k_table_scan(BatchDev* Bp) {
 // Graph solver: k_table_scan, then the last CTA to finish checks every
 // instance's buffers against its owner count (a shortfall asks the host for
 // memory before anything of the level is written) and builds the prefix of
-// row-emission groups (kEmitGroup owners each) over the instances.
+// row-emission items (kEmitItem owners each) over the instances.
 __global__ void k_table_scan_check(BatchDev* Bp) {
   __shared__ int s_last;
   __shared__ unsigned long long s_w[32], s_carry;
@@ -702,7 +702,9 @@ __global__ void k_table_scan_check(BatchDev* Bp) {
           I.planned = 0;
           I.status = ST_NEED_MEM;
         } else if (!sk) {
-          groups = (nw + kEmitGroup - 1) / kEmitGroup;
+          const int item = nw >= kEmitItemFrom ? kEmitItem : kEmitGroup;
+          I.emit_item = item;
+          groups = (nw + item - 1) / item;
         }
       }
     }
@@ -1178,11 +1180,13 @@ __global__ void __launch_bounds__(kCompactThreads) k_compact(BatchDev* Bp) {
 // ================================================================ row emission
 // Graph solver: the owners' rows appended to the level cache in canonical
 // order, solution test (insertInCache LTL_BS.cu:299-329).  Work items are
-// groups of kEmitGroup consecutive owners of one instance (prefix built by
-// k_table_scan_check); a warp takes one group at a time, lane per trace word,
-// so row reads and writes stay coalesced and the loads of every owner of the
-// group are in flight together.
-__global__ void k_emit(BatchDev* Bp) {
+// kEmitItem consecutive owners of one instance on large levels, kEmitGroup
+// on small ones (prefix built by k_table_scan_check, which records the
+// choice); a warp takes an item, each lane decodes one owner
+// (decode_level: compares with the plan's block bases), then the owners go
+// kEmitGroup at a time, lane per trace word, so row reads and writes stay
+// coalesced and the loads of a group's owners are in flight together.
+__global__ void __launch_bounds__(256, 3) k_emit(BatchDev* Bp) {
   step_entry();
   const BatchDev B = *Bp;
   const unsigned long long total = B.win_prefix[B.ninst];
@@ -1194,58 +1198,64 @@ __global__ void k_emit(BatchDev* Bp) {
     InstDev& I = B.inst[b];
     if (I.status != ST_RUNNING) continue;
     const int k = I.level, T = I.T, TP = I.TP;
-    const uint64_t o0 = (item - B.win_prefix[b]) * kEmitGroup;
+    const uint64_t per = (uint64_t)I.emit_item;
+    const uint64_t o0 = (item - B.win_prefix[b]) * per;
     const uint64_t nwin = I.n_wins;
-    // lanes 0..kEmitGroup-1 decode one owner each
+    const int cnt = (int)(nwin - o0 < per ? nwin - o0 : per);
+    // lane l decodes owner o0 + l
     int op = -1;
     const uint64_t* pa = nullptr;
     const uint64_t* pb = nullptr;
     uint64_t g = 0;
-    if (lane < kEmitGroup && o0 + lane < nwin) {
+    if (lane < cnt) {
       g = __ldcg(I.wins + o0 + lane);
-      const Cand cd = decode(I, k, g);
+      const Cand cd = decode_level(I, k, g);
       op = cd.op;
       if (op >= 0) {
         pa = row_ptr(I, cd.la, cd.a);
         pb = (op == OP_AND || op == OP_OR || op == OP_U) ? row_ptr(I, cd.lb, cd.b) : pa;
       }
     }
-    int ops[kEmitGroup];
-    const uint64_t* ra[kEmitGroup];
-    const uint64_t* rb[kEmitGroup];
-    bool bad[kEmitGroup];
-#pragma unroll
-    for (int u = 0; u < kEmitGroup; ++u) {
-      ops[u] = __shfl_sync(0xffffffffu, op, u);
-      ra[u] = (const uint64_t*)__shfl_sync(0xffffffffu, (unsigned long long)pa, u);
-      rb[u] = (const uint64_t*)__shfl_sync(0xffffffffu, (unsigned long long)pb, u);
-      bad[u] = false;
-    }
     const uint64_t r0 = I.lstart[k] + o0;
-    for (int t = lane; t < TP; t += 32) {
-      const int L = t < T ? I.len[t] : 0;
-      const uint64_t lab = (t < T && is_pos(I, t)) ? 1ULL : 0ULL;
-      uint64_t xa[kEmitGroup], xb[kEmitGroup];
+    for (int s0 = 0; s0 < cnt; s0 += kEmitGroup) {
+      int ops[kEmitGroup];
+      const uint64_t* ra[kEmitGroup];
+      const uint64_t* rb[kEmitGroup];
+      bool bad[kEmitGroup];
 #pragma unroll
       for (int u = 0; u < kEmitGroup; ++u) {
-        xa[u] = (ops[u] >= 0 && t < T) ? __ldg(ra[u] + t) : 0ULL;
-        xb[u] = (ops[u] >= 0 && t < T) ? __ldg(rb[u] + t) : 0ULL;
+        const int src = s0 + u;
+        const int o = __shfl_sync(0xffffffffu, op, src & 31);
+        ops[u] = src < cnt ? o : -1;
+        ra[u] = (const uint64_t*)__shfl_sync(0xffffffffu, (unsigned long long)pa, src & 31);
+        rb[u] = (const uint64_t*)__shfl_sync(0xffffffffu, (unsigned long long)pb, src & 31);
+        bad[u] = false;
+      }
+      for (int t = lane; t < TP; t += 32) {
+        const int L = t < T ? I.len[t] : 0;
+        const uint64_t lab = (t < T && is_pos(I, t)) ? 1ULL : 0ULL;
+        uint64_t xa[kEmitGroup], xb[kEmitGroup];
+#pragma unroll
+        for (int u = 0; u < kEmitGroup; ++u) {
+          xa[u] = (ops[u] >= 0 && t < T) ? __ldg(ra[u] + t) : 0ULL;
+          xb[u] = (ops[u] >= 0 && t < T) ? __ldg(rb[u] + t) : 0ULL;
+        }
+#pragma unroll
+        for (int u = 0; u < kEmitGroup; ++u) {
+          if (ops[u] < 0) continue;
+          const uint64_t word = t < T ? apply_w(ops[u], xa[u], xb[u], L) : 0ULL;
+          if (t < T) bad[u] |= ((word ^ lab) & 1ULL) != 0;
+          I.rows[(r0 + s0 + u) * (uint64_t)TP + t] = word;
+        }
       }
 #pragma unroll
       for (int u = 0; u < kEmitGroup; ++u) {
         if (ops[u] < 0) continue;
-        const uint64_t word = t < T ? apply_w(ops[u], xa[u], xb[u], L) : 0ULL;
-        if (t < T) bad[u] |= ((word ^ lab) & 1ULL) != 0;
-        I.rows[(r0 + u) * (uint64_t)TP + t] = word;
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < kEmitGroup; ++u) {
-      if (ops[u] < 0) continue;
-      const bool sol = !__any_sync(0xffffffffu, bad[u]);
-      if (lane == u) {
-        I.origin[r0 + u] = g;
-        if (sol) atomicMin(&I.best_sol, (unsigned long long)g);
+        const bool sol = !__any_sync(0xffffffffu, bad[u]);
+        if (lane == s0 + u) {
+          I.origin[r0 + s0 + u] = g;
+          if (sol) atomicMin(&I.best_sol, (unsigned long long)g);
+        }
       }
     }
   }
@@ -1407,6 +1417,15 @@ __global__ void k_init(BatchDev* Bp) {
     InstDev& I = B.inst[b];
     if (I.status != ST_RUNNING || I.level != 1) continue;
     if (threadIdx.x == 0) { s_first = ~0ULL; s_new = 0; }
+    if (I.atoms_staged) {
+      if (!B.atoms) {   // (never: the host uploads them before this launch)
+        __syncthreads();
+        if (threadIdx.x == 0) I.status = ST_ERROR;
+        continue;
+      }
+      const uint64_t nw = (uint64_t)I.A * I.TP;
+      for (uint64_t w = threadIdx.x; w < nw; w += blockDim.x) I.rows[w] = B.atoms[I.atom_off + w];
+    }
     __syncthreads();
     for (int v = threadIdx.x; v < I.A; v += blockDim.x) {
       const uint64_t* row = I.rows + (uint64_t)v * I.TP;

@@ -16,7 +16,11 @@ constexpr int kCompactThreads = 256;  // threads per k_compact CTA (two bitmap w
 constexpr int kAdvanceThreads = 256;
 constexpr int kTickets = 8;            // words of BatchDev::tickets
 constexpr int kTicketP1Blocks = 4;     // tickets[4]: CTAs the step's k_p1 runs (0: all), set by k_advance
-constexpr int kEmitGroup = 4;         // owners per warp step of k_emit
+constexpr int kEmitGroup = 4;         // owners per warp step of k_emit (their loads in flight together)
+constexpr int kEmitItem = 32;         // owners per k_emit work item on large levels (one warp; a lane
+                                      // decodes each); small levels take kEmitGroup per item so that
+                                      // their few owners still spread over many warps
+constexpr unsigned long long kEmitItemFrom = 1ULL << 18;   // owners from which items are kEmitItem
 
 // Global batch descriptor, resident in device memory so that buffer growth
 // never invalidates a captured launch sequence.
@@ -37,6 +41,8 @@ struct BatchDev {
                                         // compaction ticket, (unused), P1 CTAs of the step
   int2* status_out;                     // [ninst] (status, need) mirror for the host
   unsigned long long* loop_iter;        // level steps run by the current device-side loop
+  const uint64_t* atoms;                // proposition rows of the call's new instances (one upload),
+                                        // copied into each level cache by k_init
   unsigned int* ctl;                    // persistent solver: [0] barrier arrivals, [1] barrier
                                         // generation, [2] error, [3] continue flag
 };

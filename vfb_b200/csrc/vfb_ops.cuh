@@ -276,6 +276,51 @@ __device__ inline Cand decode(const InstDev& I, int k, uint64_t g) {
   return c;
 }
 
+// decode() for a candidate of the level being planned or built (k =
+// I.level) with unit costs: the block is found by comparing g with the block
+// bases the plan recorded (base_not, base_and / base_or by split, base_x,
+// base_f, base_g, base_u by split), then one division splits a pair index.
+// Same numbering as decode(); weighted levels take decode().
+__device__ inline Cand decode_level(const InstDev& I, int k, uint64_t g) {
+  if (I.weighted) return decode(I, k, g);
+  const uint64_t* n = I.lcount;
+  Cand c;
+  c.lb = 0;
+  c.b = 0;
+  const int ns = (k - 1) / 2;   // & and | splits: left sizes 1..ns
+  if (g < I.base_x) {
+    if (ns == 0 || g < I.base_and[1]) {
+      c.op = OP_NOT; c.la = k - 1; c.a = g - I.base_not;
+      return c;
+    }
+    const bool orb = g >= I.base_or[1];
+    const uint64_t* base = orb ? I.base_or : I.base_and;
+    int i = 1;
+    while (i < ns && g >= base[i + 1]) ++i;
+    c.op = orb ? OP_OR : OP_AND;
+    c.la = i;
+    c.lb = k - 1 - i;
+    divmod64(g - base[i], n[k - 1 - i], c.a, c.b);
+    return c;
+  }
+  c.la = k - 1;
+  if (g < I.base_f) { c.op = OP_X; c.a = g - I.base_x; return c; }
+  if (g < I.base_g) { c.op = OP_F; c.a = g - I.base_f; return c; }
+  if (k < 3 || g < I.base_u[1]) {
+    if (g - I.base_g < n[k - 1]) { c.op = OP_G; c.a = g - I.base_g; return c; }
+    c.op = -1; c.la = 1; c.a = 0;
+    return c;
+  }
+  int i = 1;
+  while (i < k - 2 && g >= I.base_u[i + 1]) ++i;
+  c.op = OP_U;
+  c.la = i;
+  c.lb = k - 1 - i;
+  divmod64(g - I.base_u[i], n[k - 1 - i], c.a, c.b);
+  if (c.a >= n[i]) { c.op = -1; c.la = 1; c.a = 0; c.lb = 0; c.b = 0; }
+  return c;
+}
+
 __device__ __forceinline__ const uint64_t* row_ptr(const InstDev& I, int lvl, uint64_t idx) {
   return I.rows + (I.lstart[lvl] + idx) * (uint64_t)I.TP;
 }
