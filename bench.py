@@ -39,7 +39,8 @@ cpu_baseline  the CPU restatement (single thread) on a bounded sample: the
 Extra keys of the line: "large_seed2" (the shape's own seed), "batched" (the
 256-instance mixed batch against 256 serial solves), "large_instance" (per-
 kernel profile of the mixed batch's largest instance), "serving" (the Poisson
-request stream, 2000 requests per rate, p50/p95/p99), "reference_cuda" (the
+request stream, 2000 requests per rate, p50/p95/p99; 50 req/s is replayed
+twice so that the line shows how much its tail moves between runs), "reference_cuda" (the
 reference's LTL_BS built for this GPU, timed on the planted 20+20 instance
 where its recorded runs completed).
 
@@ -72,7 +73,7 @@ WORKLOAD = ("large planted instance, deep seed: 8 APs, 31+32 traces of length 64
 METRIC = "unique characteristic sets per second (cached bottom-up LTL search, time-to-formula)"
 UNIT = "unique CS/s"
 SAMPLE_SIZE = 8      # CPU legs: the instance searched to this size
-SERVE_RATES = "500,200,100,50"
+SERVE_RATES = "500,200,100,50,50"   # 50 req/s twice: the tails' run-to-run spread
 
 
 def _peaks():
