@@ -116,7 +116,8 @@ struct InstDev {
   uint64_t base_not, base_x, base_f, base_g;
   uint64_t base_and[kMaxSize + 1], base_or[kMaxSize + 1];   // indexed by the left operand's level
   uint64_t base_u[kMaxSize];
-  // P1 tile groups: group 0 = unary over level k-1, group s = split s
+  // P1 tile groups.  Unit costs: groups 0..m-1 = the size splits (i, k-1-i),
+  // i = 1..m, then group m = the unary operators over level k-1
   uint64_t grp_prefix[kGroups + 1];
   uint32_t grp_qtiles[kGroups];
   // group g: kind 0 = unary over level la (mask bits ~ X F G), kind 1 = binary
@@ -157,6 +158,12 @@ struct InstDev {
   unsigned long long built_cands, built_wins, built_scanned;
   int built_sol_known;
   int emit_item;                 // owners per k_emit work item at this level (set by the table scan)
+  // First rows of each stored level whose ~ / X / F / G candidates satisfy
+  // the sample (step 0 of every trace equal to its label), stored as
+  // 0xFFFFFFFF - row (0: none, so a zeroed record has none); written when
+  // the level's rows are (k_init, k_emit), read by the plan of the levels
+  // that apply those operators to it
+  uint32_t uhit[kMaxSize + 2][4];
   // ---- result
   int res_size, rpn_len;
   int16_t rpn[kMaxSize];

@@ -61,6 +61,13 @@ __device__ void plan_one(InstDev& I) {
   const uint64_t keys = I.keys, table_cap = I.table_mask + 1, bitmap_words = I.bitmap_words,
                  row_cap = I.row_cap, tent_cap = I.tent_cap, promote_above = I.promote_above;
   const int attempt = I.attempt, attempt_level = I.attempt_level, rows_deferred = I.rows_deferred;
+  const int no_mask = (attempt_level == k) ? I.no_mask : 0, mask_off = I.mask_off;
+  // the first operand rows whose ~ X F G candidates satisfy the sample
+  // (recorded when those rows were written)
+  const int ulev[4] = {Ln, k - wX, k - wF, k - wG};
+  uint32_t uh[4];
+#pragma unroll
+  for (int o = 0; o < 4; ++o) uh[o] = ulev[o] >= c1 ? I.uhit[ulev[o]][o] : 0u;
   const uint64_t lstart_k = lstart_prev + n[k - 1];
   I.lstart[k] = lstart_k;
   // candidate blocks in canonical order: ~ & | X F G U; a unary operator of
@@ -118,17 +125,22 @@ __device__ void plan_one(InstDev& I) {
       for (int u = 0; u < 6; ++u) tl[u] += st * ((nQ + (1ULL << u) - 1) >> u);
     }
   };
+  // unit costs: one group per size split, then one unary group over level
+  // k-1.  The unary group comes last so that a solution among the & | blocks,
+  // which precede X F G in the candidate order, is known before its tiles
+  // start: they then compute ~ alone.
+  const int msplit = (k - 1) / 2;
+  auto u_kind = [&](int q) { return q < msplit ? 1 : 0; };
+  auto u_la = [&](int q) { return q < msplit ? q + 1 : k - 1; };
+  auto u_lb = [&](int q) { return q < msplit ? k - 2 - q : 0; };
+  auto u_mask = [&](int q) { return q < msplit ? (2 * (q + 1) == k - 1 ? 7 : 15) : 0xF; };
   if (!weighted) {
-    // unit costs: one unary group over level k-1, one group per size split
-    I.grp_kind[0] = 0; I.grp_la[0] = (uint8_t)(k - 1); I.grp_lb[0] = 0; I.grp_mask[0] = 0xF;
-    add_tiles(0, k - 1, 0);
-    ng = 1;
-    for (int i = 1; 2 * i <= k - 1; ++i, ++ng) {
-      I.grp_kind[ng] = 1;
-      I.grp_la[ng] = (uint8_t)i;
-      I.grp_lb[ng] = (uint8_t)(k - 1 - i);
-      I.grp_mask[ng] = (uint8_t)(i == k - 1 - i ? 7 : 15);
-      add_tiles(1, i, k - 1 - i);
+    for (ng = 0; ng <= msplit; ++ng) {
+      I.grp_kind[ng] = (uint8_t)u_kind(ng);
+      I.grp_la[ng] = (uint8_t)u_la(ng);
+      I.grp_lb[ng] = (uint8_t)u_lb(ng);
+      I.grp_mask[ng] = (uint8_t)u_mask(ng);
+      add_tiles(u_kind(ng), u_la(ng), u_lb(ng));
     }
   } else {
     // weighted: a level (pair) may serve several operators, so the groups
@@ -173,10 +185,10 @@ __device__ void plan_one(InstDev& I) {
   // operator bases of every group (what a P1 tile needs to tell whether an
   // operator's candidates can still come before the best solution found)
   for (int q = 0; q < ng; ++q) {
-    const int kind = weighted ? I.grp_kind[q] : (q > 0);
-    const int mask = weighted ? I.grp_mask[q] : (q == 0 ? 0xF : (2 * q == k - 1 ? 7 : 15));
-    const int la = weighted ? I.grp_la[q] : (q ? q : k - 1);
-    const int lb = weighted ? I.grp_lb[q] : (q ? k - 1 - q : 0);
+    const int kind = weighted ? I.grp_kind[q] : u_kind(q);
+    const int mask = weighted ? I.grp_mask[q] : u_mask(q);
+    const int la = weighted ? I.grp_la[q] : u_la(q);
+    const int lb = weighted ? I.grp_lb[q] : u_lb(q);
     uint64_t b4[4];
     if (kind == 0) {
       b4[0] = 0;   // ~ is the first block
@@ -212,9 +224,9 @@ __device__ void plan_one(InstDev& I) {
     uint64_t acc = 0;
     I.grp_prefix[0] = 0;
     for (int q = 0; q < ng; ++q) {
-      const int kind = weighted ? I.grp_kind[q] : (q > 0);
-      const int la = weighted ? I.grp_la[q] : (q ? q : k - 1);
-      const int lb = weighted ? I.grp_lb[q] : (q ? k - 1 - q : 0);
+      const int kind = weighted ? I.grp_kind[q] : u_kind(q);
+      const int la = weighted ? I.grp_la[q] : u_la(q);
+      const int lb = weighted ? I.grp_lb[q] : u_lb(q);
       if (kind == 0) {
         acc += (n[la] + kTS - 1) / kTS;
       } else {
@@ -261,7 +273,23 @@ __device__ void plan_one(InstDev& I) {
     I.p1_step = t;
     I.p1_tail = 1;
     I.n_new = I.n_wins = I.probe_fail = I.n_newlist = 0;
-    I.best_cand = I.best_sol = ~0ULL;
+    // A unary candidate recorded as satisfying the sample bounds the level's
+    // first solution from the start, as if a P1 tile had found it: operators
+    // past it are skipped everywhere (not in a full re-run, nor where the
+    // level cannot be re-run)
+    uint64_t first = ~0ULL;
+    if (!no_mask && !mask_off) {
+      const uint64_t ub[4] = {0, bx[0], bx[1], bx[2]};
+#pragma unroll
+      for (int o = 0; o < 4; ++o) {
+        const uint64_t row = 0xFFFFFFFFull - uh[o];
+        if (uh[o] && row < n[ulev[o]] && ub[o] + row < first) first = ub[o] + row;
+      }
+    }
+    I.best_cand = first;
+    I.best_sol = ~0ULL;
+#pragma unroll
+    for (int o = 0; o < 4; ++o) I.uhit[k][o] = 0u;   // (this level's rows are written after it)
     I.sol_known = 0;
     I.p1_masked = 0;
     if (attempt_level != k) I.no_mask = 0;   // a new level may skip again
@@ -503,15 +531,18 @@ __device__ void ph_p1(const BatchDev& B) {
       const int keys = (P.mask & 8) ? 15 : (P.mask & 4) ? 7 : 3;
       switch (P.mode) {
         case KEY_HASH:
-          if (P.kind == 0) p1_unary<KEY_HASH, BULK>(I, P, sS, sp, cnt);
+          if (P.kind == 0 && P.mask == 1) p1_unary<KEY_HASH, BULK, 1>(I, P, sS, sp, cnt);
+          else if (P.kind == 0) p1_unary<KEY_HASH, BULK, 4>(I, P, sS, sp, cnt);
           else p1_binary_keys<KEY_HASH, BULK>(keys, I, P, sS, sp, sQ, cnt);
           break;
         case KEY_SAMPLED:
-          if (P.kind == 0) p1_unary<KEY_SAMPLED, BULK>(I, P, sS, sp, cnt);
+          if (P.kind == 0 && P.mask == 1) p1_unary<KEY_SAMPLED, BULK, 1>(I, P, sS, sp, cnt);
+          else if (P.kind == 0) p1_unary<KEY_SAMPLED, BULK, 4>(I, P, sS, sp, cnt);
           else p1_binary_keys<KEY_SAMPLED, BULK>(keys, I, P, sS, sp, sQ, cnt);
           break;
         default:
-          if (P.kind == 0) p1_unary<KEY_CONCAT, BULK>(I, P, sS, sp, cnt);
+          if (P.kind == 0 && P.mask == 1) p1_unary<KEY_CONCAT, BULK, 1>(I, P, sS, sp, cnt);
+          else if (P.kind == 0) p1_unary<KEY_CONCAT, BULK, 4>(I, P, sS, sp, cnt);
           else p1_binary_keys<KEY_CONCAT, BULK>(keys, I, P, sS, sp, sQ, cnt);
       }
     }
@@ -1221,7 +1252,7 @@ __global__ void __launch_bounds__(256, 3) k_emit(BatchDev* Bp) {
       int ops[kEmitGroup];
       const uint64_t* ra[kEmitGroup];
       const uint64_t* rb[kEmitGroup];
-      bool bad[kEmitGroup];
+      unsigned miss[kEmitGroup];   // emit_miss OR-ed over the words
 #pragma unroll
       for (int u = 0; u < kEmitGroup; ++u) {
         const int src = s0 + u;
@@ -1229,11 +1260,12 @@ __global__ void __launch_bounds__(256, 3) k_emit(BatchDev* Bp) {
         ops[u] = src < cnt ? o : -1;
         ra[u] = (const uint64_t*)__shfl_sync(0xffffffffu, (unsigned long long)pa, src & 31);
         rb[u] = (const uint64_t*)__shfl_sync(0xffffffffu, (unsigned long long)pb, src & 31);
-        bad[u] = false;
+        miss[u] = 0u;
       }
       for (int t = lane; t < TP; t += 32) {
         const int L = t < T ? I.len[t] : 0;
-        const uint64_t lab = (t < T && is_pos(I, t)) ? 1ULL : 0ULL;
+        const unsigned lab = (t < T && is_pos(I, t)) ? 1u : 0u;
+        const uint64_t lm = len_mask(L);
         uint64_t xa[kEmitGroup], xb[kEmitGroup];
 #pragma unroll
         for (int u = 0; u < kEmitGroup; ++u) {
@@ -1244,17 +1276,18 @@ __global__ void __launch_bounds__(256, 3) k_emit(BatchDev* Bp) {
         for (int u = 0; u < kEmitGroup; ++u) {
           if (ops[u] < 0) continue;
           const uint64_t word = t < T ? apply_w(ops[u], xa[u], xb[u], L) : 0ULL;
-          if (t < T) bad[u] |= ((word ^ lab) & 1ULL) != 0;
+          if (t < T) miss[u] |= emit_miss(word, lm, lab);
           I.rows[(r0 + s0 + u) * (uint64_t)TP + t] = word;
         }
       }
 #pragma unroll
       for (int u = 0; u < kEmitGroup; ++u) {
         if (ops[u] < 0) continue;
-        const bool sol = !__any_sync(0xffffffffu, bad[u]);
+        const unsigned m = __reduce_or_sync(0xffffffffu, miss[u]);
         if (lane == s0 + u) {
           I.origin[r0 + s0 + u] = g;
-          if (sol) atomicMin(&I.best_sol, (unsigned long long)g);
+          if (!(m & 1u)) atomicMin(&I.best_sol, (unsigned long long)g);
+          record_unary(I, k, o0 + s0 + u, ((m >> 4) & 1u) | (m & 0xEu));   // (~ X F G)
         }
       }
     }
@@ -1416,7 +1449,11 @@ __global__ void k_init(BatchDev* Bp) {
   for (int b = blockIdx.x; b < B.ninst; b += gridDim.x) {
     InstDev& I = B.inst[b];
     if (I.status != ST_RUNNING || I.level != 1) continue;
-    if (threadIdx.x == 0) { s_first = ~0ULL; s_new = 0; }
+    if (threadIdx.x == 0) {
+      s_first = ~0ULL;
+      s_new = 0;
+      for (int o = 0; o < 4; ++o) I.uhit[atom_level(I)][o] = 0u;
+    }
     if (I.atoms_staged) {
       if (!B.atoms) {   // (never: the host uploads them before this launch)
         __syncthreads();
@@ -1439,8 +1476,14 @@ __global__ void k_init(BatchDev* Bp) {
       if (isnew) atomicAdd(&s_new, 1ULL);
       I.origin[v] = v;
       bool sol = true;
-      for (int t = 0; t < I.T; ++t) sol = sol && (((row[t] & 1ULL) != 0) == is_pos(I, t));
+      unsigned miss = 0u;
+      for (int t = 0; t < I.T; ++t) {
+        const unsigned lab = is_pos(I, t) ? 1u : 0u;
+        sol = sol && (((row[t] & 1ULL) != 0) == (lab != 0));
+        miss |= unary_miss(row[t], len_mask(I.len[t]), lab);
+      }
       if (sol) atomicMin(&s_first, (unsigned long long)v);
+      record_unary(I, atom_level(I), (uint64_t)v, miss);
     }
     __syncthreads();
     if (threadIdx.x == 0) {

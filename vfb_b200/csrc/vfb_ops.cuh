@@ -509,45 +509,87 @@ __device__ __forceinline__ void p1_words(const TileSh& P, F&& body) {
 // with the trace's label, so 32 bits carry the whole test.
 __device__ __forceinline__ uint32_t lo32(uint64_t w) { return (uint32_t)w; }
 
+// Step 0 of ~w, X w, F w and G w on one trace word (length mask lm) against
+// the trace's label: bit o set (o = ~ X F G) where it differs.  The same
+// bits as the P1 tests of ~w & lm, w >> 1, w_fin(w) and w_glob(w, lm); a row
+// whose bits stay clear over every trace makes that operator's candidate on
+// it a solution.
+__device__ __forceinline__ unsigned unary_miss(uint64_t w, uint64_t lm, unsigned lab) {
+  const unsigned n0 = (unsigned)(~w & lm) & 1u;
+  const unsigned x0 = (unsigned)(w >> 1) & 1u;
+  const unsigned f0 = w != 0 ? 1u : 0u;
+  const unsigned g0 = ((w & 1ULL) != 0 && (~w & lm) == 0) ? 1u : 0u;
+  return (n0 ^ lab) | ((x0 ^ lab) << 1) | ((f0 ^ lab) << 2) | ((g0 ^ lab) << 3);
+}
+
+// The step-0 tests of k_emit on one word of a row, trace lengths being at
+// least 1 (so ~w passes exactly where w fails, and G w at step 0 is the word
+// covering the whole trace): bit 0 = the row's own test missed, bits 1-4 =
+// X, F, G, ~ missed.  OR-ed over the words they are the row's miss bits.
+__device__ __forceinline__ unsigned emit_miss(uint64_t w, uint64_t lm, unsigned lab) {
+  const unsigned x = ((unsigned)w ^ (lab ? 3u : 0u)) & 3u;
+  const unsigned nz = w != 0 ? 1u : 0u;
+  const unsigned fu = (~w & lm) == 0 ? 1u : 0u;
+  return x | ((nz ^ lab) << 2) | ((fu ^ lab) << 3) | ((~x & 1u) << 4);
+}
+
+// Records row `row` of level k as the first one found so far whose ~ X F G
+// candidates pass the sample, for the operators whose miss bits are clear.
+__device__ __forceinline__ void record_unary(InstDev& I, int k, uint64_t row, unsigned miss) {
+  if ((miss & 0xFu) == 0xFu || row >= 0xFFFFFFFFull) return;
+  const unsigned v = (unsigned)(0xFFFFFFFFull - row);
+#pragma unroll
+  for (int o = 0; o < 4; ++o)
+    if (!((miss >> o) & 1u)) atomicMax(&I.uhit[k][o], v);
+}
+
 // BULK: rows staged by one bulk copy at the even pitch TP (rotated word
 // order), else by 8-byte copies at the odd pitch TP + 1.
-template <int MODE, bool BULK>
+// NU: the operators computed, ~ alone (1: every other one lies past the
+// level's first solution) or ~ X F G (4; the inserted ones are P.mask).
+template <int MODE, bool BULK, int NU>
 __device__ inline void p1_unary(InstDev& I, const TileSh& P, const uint64_t* sS, int sp, P1Count& cnt) {
   const uint64_t a = P.s0 + threadIdx.x;
   const unsigned live = __ballot_sync(0xffffffffu, a < P.nS);
   if (a >= P.nS) return;
   const uint64_t* srow = sS + threadIdx.x * sp;
   KeyAcc k0, k1, k2, k3;
-  key_init(k0); key_init(k1); key_init(k2); key_init(k3);
+  key_init(k0);
+  if (NU == 4) { key_init(k1); key_init(k2); key_init(k3); }
   uint32_t bad[4] = {0, 0, 0, 0};
   auto body = [&](int t, auto half) {
     const uint64_t w = srow[t];
     const int L = P.len[t], off = P.off[t], wd = P.wid[t];
     const uint64_t lm = len_mask(L);
     const uint32_t pb = (uint32_t)pos_bit(P, t);
-    const uint64_t w0 = ~w & lm, w1 = w >> 1, w2 = w_fin(w), w3 = w_glob(w, lm);
+    const uint64_t w0 = ~w & lm;
     bad[0] |= lo32(w0) ^ pb;
-    bad[1] |= lo32(w1) ^ pb;
-    bad[2] |= lo32(w2) ^ pb;
-    bad[3] |= lo32(w3) ^ pb;
     key_word_any<MODE>(k0, w0, t, half, off, wd, P.stride, L);
-    key_word_any<MODE>(k1, w1, t, half, off, wd, P.stride, L);
-    key_word_any<MODE>(k2, w2, t, half, off, wd, P.stride, L);
-    key_word_any<MODE>(k3, w3, t, half, off, wd, P.stride, L);
+    if (NU == 4) {
+      const uint64_t w1 = w >> 1, w2 = w_fin(w), w3 = w_glob(w, lm);
+      bad[1] |= lo32(w1) ^ pb;
+      bad[2] |= lo32(w2) ^ pb;
+      bad[3] |= lo32(w3) ^ pb;
+      key_word_any<MODE>(k1, w1, t, half, off, wd, P.stride, L);
+      key_word_any<MODE>(k2, w2, t, half, off, wd, P.stride, L);
+      key_word_any<MODE>(k3, w3, t, half, off, wd, P.stride, L);
+    }
   };
   p1_words<BULK>(P, body);
   uint64_t h[4], l[4], g[4];
   key_final<MODE>(k0, h[0], l[0]);
-  key_final<MODE>(k1, h[1], l[1]);
-  key_final<MODE>(k2, h[2], l[2]);
-  key_final<MODE>(k3, h[3], l[3]);
   g[0] = I.base_not + a;
-  g[1] = I.base_x + a;
-  g[2] = I.base_f + a;
-  g[3] = I.base_g + a;
+  if (NU == 4) {
+    key_final<MODE>(k1, h[1], l[1]);
+    key_final<MODE>(k2, h[2], l[2]);
+    key_final<MODE>(k3, h[3], l[3]);
+    g[1] = I.base_x + a;
+    g[2] = I.base_f + a;
+    g[3] = I.base_g + a;
+  }
 #pragma unroll
   for (int j = 0; j < 4; ++j) bad[j] &= 1u;
-  insert_group<4>(I, live, P.k, h, l, g, bad, cnt, (unsigned)P.mask);
+  insert_group<NU>(I, live, P.k, h, l, g, bad, cnt, (unsigned)P.mask);
 }
 
 // KEYS: the operators computed, a prefix of (&, |, laUlb, lbUla) as bits
