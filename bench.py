@@ -39,8 +39,9 @@ cpu_baseline  the CPU restatement (single thread) on a bounded sample: the
 Extra keys of the line: "large_seed2" (the shape's own seed), "batched" (the
 256-instance mixed batch against 256 serial solves), "large_instance" (per-
 kernel profile of the mixed batch's largest instance), "serving" (the Poisson
-request stream, 2000 requests per rate, p50/p95/p99; 50 req/s is replayed
-twice so that the line shows how much its tail moves between runs), "reference_cuda" (the
+request stream, 2000 requests per rate, p50/p95/p99, engine budget 64 GiB;
+500 req/s is replayed twice so that the line shows how much its tail moves
+between runs), "reference_cuda" (the
 reference's LTL_BS built for this GPU, timed on the planted 20+20 instance
 where its recorded runs completed).
 
@@ -73,7 +74,8 @@ WORKLOAD = ("large planted instance, deep seed: 8 APs, 31+32 traces of length 64
 METRIC = "unique characteristic sets per second (cached bottom-up LTL search, time-to-formula)"
 UNIT = "unique CS/s"
 SAMPLE_SIZE = 8      # CPU legs: the instance searched to this size
-SERVE_RATES = "500,200,100,50,50"   # 50 req/s twice: the tails' run-to-run spread
+SERVE_RATES = "500,500,200,100,50"   # 500 req/s twice: the tails' run-to-run spread
+SERVE_MEM_BYTES = 64 << 30          # serving engine budget (a quarter of it per request)
 
 
 def _peaks():
@@ -382,7 +384,7 @@ def serving(local: int, rates: str, count: int):
     replayed in real time at each rate through the continuous-batching loop."""
     import vfb_b200
     from vfb_b200 import serve, synth
-    eng = vfb_b200.Engine(device=local)
+    eng = vfb_b200.Engine(device=local, mem_limit_bytes=SERVE_MEM_BYTES)
     eng.serve_limits(0.8, 0, 1 << 25)
     out = []
     for rate in [float(x) for x in rates.split(",") if x]:
@@ -394,7 +396,8 @@ def serving(local: int, rates: str, count: int):
         out.append(serve.summarize(rate, res, lat, span, 256, large))
     eng.close()
     return {"workload": f"Poisson request stream, seed 4, {count} requests per rate; 95% mixed-batch shapes, "
-                        "5% the large shape (own seeds, max size 17, per-request cap a quarter of the budget)",
+                        "5% the large shape (own seeds, max size 17); engine budget "
+                        f"{SERVE_MEM_BYTES >> 30} GiB, per-request cap a quarter of it",
             "rates": out,
             "not_run": "rates 20 and 10 req/s (100 s and 200 s of arrivals): python bench.py --serve-rates 20,10"}
 

@@ -194,7 +194,12 @@ vfb_status vfb_solve_noalloc(const vfb_instance *inst, vfb_result *out);
  * the others' steps for long.  vfb_serve_limits sets budget_frac (default
  * 0.8), request_bytes (0, the default: a quarter of the budget) and
  * step_candidates (default 2^25; 0: whole levels) for the next
- * vfb_serve_open and the open session. */
+ * vfb_serve_open and the open session.  vfb_serve_open takes the memory
+ * budget (less what the engine holds live) from the device in one
+ * allocation, halved until it can be had, and the session's buffers are
+ * carved out of it, so that growth inside a step maps no new device memory;
+ * vfb_serve_close gives it back to the engine's pool (vfb_destroy returns
+ * the pool's memory to the device). */
 typedef struct {
   uint64_t tag;
   vfb_result result;

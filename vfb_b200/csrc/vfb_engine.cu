@@ -137,6 +137,50 @@ struct Engine {
   size_t cached_bytes = 0;  // blocks in free_blocks
   size_t peak_live = 0;     // most bytes live at once since the last trim
 
+  // Serving arena: a serving session carves its blocks out of one device
+  // allocation made when the session opens.  A cudaMallocAsync that has to
+  // map fresh memory costs about 10 ms per GB on a B200, and a growth inside
+  // a serve step would wait for it while every request of the step waits too.
+  // Free ranges are kept by offset; a block takes the smallest range that
+  // fits and a released block merges with its free neighbours.  Every user of
+  // a block runs on the engine's one stream, so a range released after its
+  // last launch is only handed to launches enqueued after that.
+  struct Arena {
+    char* base = nullptr;
+    size_t size = 0;
+    std::map<size_t, size_t> free_ranges;   // offset -> bytes
+
+    bool owns(const void* p) const {
+      return base && (const char*)p >= base && (const char*)p < base + size;
+    }
+    void* take(size_t bytes) {
+      auto best = free_ranges.end();
+      for (auto it = free_ranges.begin(); it != free_ranges.end(); ++it)
+        if (it->second >= bytes && (best == free_ranges.end() || it->second < best->second)) best = it;
+      if (best == free_ranges.end()) return nullptr;
+      const size_t off = best->first, len = best->second;
+      free_ranges.erase(best);
+      if (len > bytes) free_ranges.emplace(off + bytes, len - bytes);
+      return base + off;
+    }
+    void give(void* p, size_t bytes) {
+      size_t off = (size_t)((char*)p - base), len = bytes;
+      auto next = free_ranges.lower_bound(off);
+      if (next != free_ranges.end() && off + len == next->first) {
+        len += next->second;
+        next = free_ranges.erase(next);
+      }
+      if (next != free_ranges.begin()) {
+        auto prev = std::prev(next);
+        if (prev->first + prev->second == off) {
+          prev->second += len;
+          return;
+        }
+      }
+      free_ranges.emplace(off, len);
+    }
+  } arena;
+
   // per-call counters
   uint64_t c_h2d = 0, c_d2h = 0, c_launch = 0;
   cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr;
@@ -171,9 +215,17 @@ struct Engine {
     free_workspace();
     for (auto& kv : free_blocks) cudaFree(kv.second);
     free_blocks.clear();
-    for (auto& kv : live_blocks) cudaFree(kv.first);
+    for (auto& kv : live_blocks)
+      if (!arena.owns(kv.first)) cudaFree(kv.first);
     live_blocks.clear();
     held_bytes = cached_bytes = 0;
+    if (arena.base) cudaFree(arena.base);
+    arena = Arena{};
+    // the device pool keeps freed memory for reuse while the engine lives
+    // (release threshold); an engine that ends gives it back to the device
+    if (stream) cudaStreamSynchronize(stream);
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
     if (h_status) cudaFreeHost(h_status);
     h_status = nullptr;
     if (h_stage) cudaFreeHost(h_stage);
@@ -218,6 +270,20 @@ struct Engine {
   // size becomes the capacity); larger cached blocks stay for larger requests.
   void* dalloc(size_t bytes, size_t* got) {
     if (bytes < 256) bytes = 256;
+    if (arena.base) {
+      // within a serving session: a range of the arena (256-byte multiples),
+      // else (no range fits) the pool below, under the same budget
+      const size_t n = (bytes + 255) & ~(size_t)255;
+      if (!mem_limit || held_bytes + n <= mem_limit) {
+        if (void* p = arena.take(n)) {
+          held_bytes += n;
+          live_blocks[p] = n;
+          *got = n;
+          peak_live = std::max(peak_live, held_bytes - cached_bytes);
+          return p;
+        }
+      }
+    }
     auto it = free_blocks.lower_bound(bytes);
     if (it != free_blocks.end() && it->first <= 4 * bytes) {
       void* p = it->second;
@@ -279,6 +345,12 @@ struct Engine {
     if (!p) return;
     auto it = live_blocks.find(p);
     if (it == live_blocks.end()) return;
+    if (arena.owns(p)) {
+      arena.give(p, it->second);
+      held_bytes -= it->second;
+      live_blocks.erase(it);
+      return;
+    }
     free_blocks.emplace(it->second, p);
     cached_bytes += it->second;
     live_blocks.erase(it);
@@ -1471,6 +1543,7 @@ struct Engine {
     sv.budget_frac = sv_budget_frac;
     sv.request_bytes = sv_request_bytes ? sv_request_bytes : (uint64_t)(mem_limit / 4);
     sv.step_cands = sv_step_cands;
+    open_arena();
     if (cudaMallocHost(&sv.h_inst, (size_t)slots * sizeof(InstDev)) != cudaSuccess) {
       sv.h_inst = nullptr;
       return VFB_OOM;
@@ -1492,11 +1565,50 @@ struct Engine {
     return VFB_OK;
   }
 
+  // The arena of a serving session: the budget less what is live, in one
+  // allocation (halved until it can be had, down to 1 GB; without one, blocks
+  // come from the pool as in a solve).  The cached blocks go back to the pool
+  // first, since the arena takes their memory.
+  void open_arena() {
+    if (arena.base) return;
+    for (auto& kv : free_blocks) cudaFreeAsync(kv.second, stream);
+    free_blocks.clear();
+    held_bytes -= cached_bytes;
+    cached_bytes = 0;
+    const size_t gran = (size_t)1 << 21;
+    size_t want = mem_limit > held_bytes ? (mem_limit - held_bytes) & ~(gran - 1) : 0;
+    void* p = nullptr;
+    while (want >= ((size_t)1 << 30)) {
+      if (cudaMallocAsync(&p, want, stream) == cudaSuccess) break;
+      cudaGetLastError();
+      p = nullptr;
+      want = (want / 2) & ~(gran - 1);
+    }
+    if (!p || cudaStreamSynchronize(stream) != cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
+    arena.base = (char*)p;
+    arena.size = want;
+    arena.free_ranges.clear();
+    arena.free_ranges.emplace(0, want);
+  }
+
+  // Gives the arena back to the pool once none of its blocks is live.
+  void close_arena() {
+    if (!arena.base) return;
+    for (auto& kv : live_blocks)
+      if (arena.owns(kv.first)) return;
+    cudaFreeAsync(arena.base, stream);
+    arena = Arena{};
+  }
+
   void serve_close() {
     for (int i = 0; i < sv.cap; ++i)
       if (sv.busy[i] && sv.H[i].d.rows) free_buffers(sv.H[i]);
     if (sv.h_inst) cudaFreeHost(sv.h_inst);
     sv = Session{};
+    close_arena();
     trim_cache();
     single_step = false;
     if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
