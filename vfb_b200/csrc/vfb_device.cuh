@@ -141,6 +141,11 @@ struct InstDev {
   unsigned long long best_cand;  // min candidate index whose CS satisfies the sample (P1)
   unsigned long long best_sol;   // min candidate index of a solution owning its key
   int sol_known;                 // best_sol settled before the rows were emitted
+  // At a level with a solution candidate the table scan counts the owners
+  // below it (n_below) instead of marking every owner's bit; counted_below:
+  // the count stands (the candidate owns its key), lcount = n_below + 1
+  unsigned long long n_below;
+  int counted_below;
   int fill;                      // 1: the table and the bitmap are still to be initialised (k_fill)
   int atoms_staged;              // 1: the proposition rows wait in the batch's staging buffer at
   uint64_t atom_off;             // word atom_off; k_init copies them into the level cache

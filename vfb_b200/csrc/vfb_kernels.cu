@@ -288,6 +288,8 @@ __device__ void plan_one(InstDev& I) {
     }
     I.best_cand = first;
     I.best_sol = ~0ULL;
+    I.n_below = 0;
+    I.counted_below = 0;
 #pragma unroll
     for (int o = 0; o < 4; ++o) I.uhit[k][o] = 0u;   // (this level's rows are written after it)
     I.sol_known = 0;
@@ -602,8 +604,15 @@ __global__ void __launch_bounds__(kTS) k_p1_bulk(BatchDev* Bp) {
 // level k.  One chunk of kScanSlots slots per CTA iteration; an empty slot's
 // payload (~0) carries no level <= 32.  One warp per instance also settles
 // whether the recorded solution candidate owns its key.
+// The table scan's counting mode at a level that has a solution candidate
+// after P1 (the fields read are not written during the scan, except no_mask
+// by a failed ownership check, which rebuilds the level anyway).
+__device__ __forceinline__ bool below_mode(const InstDev& I) {
+  return I.best_cand != ~0ULL && !I.on_the_fly && !I.no_mask && !I.mask_off;
+}
+
 __device__ void ph_table_scan(const BatchDev& B, unsigned bid, unsigned nb) {
-  __shared__ unsigned long long s_w[32];
+  __shared__ unsigned long long s_w[32], s_b[32];
   const unsigned long long total = B.tscan_prefix[B.ninst];
   for (unsigned long long c = bid; c < total; c += nb) {
     const int b = find_owner(B.tscan_prefix, B.ninst, c);
@@ -615,7 +624,14 @@ __device__ void ph_table_scan(const BatchDev& B, unsigned bid, unsigned nb) {
     const uint64_t s0 = (c - B.tscan_prefix[b]) * kScanSlots;
     const uint64_t cap = listed ? I.n_newlist : I.table_mask + 1;
     const uint64_t s1 = (s0 + kScanSlots < cap) ? s0 + kScanSlots : cap;
-    unsigned long long cnt = 0;
+    // a level with a solution candidate (where it may skip operators) counts
+    // the owners below the candidate instead of marking owner bits: if the
+    // candidate owns its key (nearly always, and always with exact keys)
+    // that count is all the level needs; if not, the level is built again in
+    // full (the ownership check below)
+    const unsigned long long bc = I.best_cand;
+    const bool below = below_mode(I);
+    unsigned long long cnt = 0, nbelow = 0;
     // kScanBatch entries per thread at a time: their list reads, then their
     // payload reads, are in flight together
     for (uint64_t e0 = s0 + threadIdx.x; e0 < s1; e0 += (uint64_t)kScanBatch * blockDim.x) {
@@ -632,18 +648,27 @@ __device__ void ph_table_scan(const BatchDev& B, unsigned bid, unsigned nb) {
       for (int u = 0; u < kScanBatch; ++u) {
         if ((pay[u] >> kPayShift) == k) {
           const uint64_t g = pay[u] & kIdxMask;
-          atomicOr(I.bitmap + (g >> 5), 1u << (g & 31));
+          if (below) nbelow += g < bc ? 1 : 0;
+          else atomicOr(I.bitmap + (g >> 5), 1u << (g & 31));
           ++cnt;
         }
       }
     }
     cnt = warp_sum(cnt);
-    if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = cnt;
+    nbelow = warp_sum(nbelow);
+    if ((threadIdx.x & 31) == 0) {
+      s_w[threadIdx.x >> 5] = cnt;
+      s_b[threadIdx.x >> 5] = nbelow;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
-      unsigned long long t = 0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_w[w];
+      unsigned long long t = 0, tb = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+        t += s_w[w];
+        tb += s_b[w];
+      }
       if (t) atomicAdd(&I.n_wins, t);
+      if (tb) atomicAdd(&I.n_below, tb);
     }
     __syncthreads();
   }
@@ -665,13 +690,16 @@ __device__ void ph_table_scan(const BatchDev& B, unsigned bid, unsigned nb) {
       default: warp_key<KEY_CONCAT>(I, cd, lane, h, l);
     }
     if (lane == 0) {
+      const bool counting = below_mode(I);
       if (find_pay(I.table, I.table_mask, h, l) == pay_of(k, g)) {
         I.best_sol = g;
         I.sol_known = 1;
-      } else if (I.p1_masked) {
+        I.counted_below = counting ? 1 : 0;
+      } else if (I.p1_masked || counting) {
         // an earlier candidate of the level shares the first solution's key
-        // (a relaxed-key collision) while operators past it were skipped: the
-        // level is built again in full (the host re-plans it, nothing to grow)
+        // (a relaxed-key collision) while operators past it were skipped or
+        // the owners were only counted: the level is built again in full (the
+        // host re-plans it, nothing to grow)
         I.no_mask = 1;
         I.need = 0;
         I.planned = 0;
@@ -963,7 +991,9 @@ __device__ void finish_one(InstDev& I) {
   const uint64_t cands = I.cands, wins = I.n_wins, newlist = I.n_newlist, tent = I.tent_cap,
                  cap = I.table_mask + 1, best = I.best_sol, keys = I.keys;
   const uint64_t* wlist = I.wins;
-  const int attempt = I.attempt, sol_known = I.sol_known, max_size = I.max_size;
+  const uint64_t n_below = I.n_below;
+  const int attempt = I.attempt, sol_known = I.sol_known, max_size = I.max_size,
+            counted_below = I.counted_below;
   I.built_cands = cands;
   I.built_wins = wins;
   I.built_scanned = (attempt == 1 && newlist <= tent) ? newlist : cap;
@@ -972,9 +1002,13 @@ __device__ void finish_one(InstDev& I) {
   if (best != ~0ULL) {
     const uint64_t g = best;
     uint64_t lo = 0, hi = wins;   // first index with wins[idx] >= g
-    while (lo < hi) {
-      const uint64_t mid = (lo + hi) >> 1;
-      if (wlist[mid] < g) lo = mid + 1; else hi = mid;
+    if (counted_below) {
+      lo = n_below;
+    } else {
+      while (lo < hi) {
+        const uint64_t mid = (lo + hi) >> 1;
+        if (wlist[mid] < g) lo = mid + 1; else hi = mid;
+      }
     }
     I.lcount[k] = lo + 1;
     I.lcands[k] = g + 1;
