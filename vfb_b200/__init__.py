@@ -192,14 +192,25 @@ class Problem:
                    list(inst.names) or [f"a{v}" for v in range(inst.num_vars)],
                    inst.max_size, inst.rlx_type, max(l for l, _ in traces))
 
+    def __setattr__(self, name, value):
+        # assigning new words or lengths drops the converted copies
+        if name in ("words", "lengths"):
+            object.__setattr__(self, "_arrays", None)
+        object.__setattr__(self, name, value)
+
     def _cstruct(self):
-        # the C arrays are Python array buffers (one C-level conversion each);
-        # the caller keeps them alive until the call returns
-        w = array.array("Q", self.words or [0])
-        ln = array.array("i", self.lengths or [0])
-        s = _Instance(self.num_vars, self.num_traces, self.num_pos,
-                      ctypes.cast(w.buffer_info()[0], _P_U64), ctypes.cast(ln.buffer_info()[0], _P_INT),
-                      self.max_size, self.rlx_type)
+        # the C arrays are Python array buffers, converted once per Problem
+        # (words and lengths are taken as fixed once a Problem has been
+        # solved: assign new lists to change them); the caller keeps them
+        # alive until the call returns
+        arrays = getattr(self, "_arrays", None)
+        if arrays is None:
+            w = array.array("Q", self.words or [0])
+            ln = array.array("i", self.lengths or [0])
+            arrays = (w, ln, ctypes.cast(w.buffer_info()[0], _P_U64), ctypes.cast(ln.buffer_info()[0], _P_INT))
+            object.__setattr__(self, "_arrays", arrays)
+        w, ln, wp, lp = arrays
+        s = _Instance(self.num_vars, len(self.lengths), self.num_pos, wp, lp, self.max_size, self.rlx_type)
         return s, (w, ln)
 
 

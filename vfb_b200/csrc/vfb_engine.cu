@@ -124,6 +124,8 @@ struct Engine {
   uint64_t* h_stage = nullptr;  // pinned upload staging
   size_t h_stage_words = 0;
   uint64_t* d_atoms = nullptr;  // device staging of a batch's proposition rows (one upload)
+  InstDev* h_recs = nullptr;    // pinned mirror of a batch's instance records (uploads, results)
+  int h_recs_cap = 0;
   size_t d_atoms_words = 0;
 
   // graphs
@@ -235,6 +237,9 @@ struct Engine {
     if (d_atoms) cudaFree(d_atoms);
     d_atoms = nullptr;
     d_atoms_words = 0;
+    if (h_recs) cudaFreeHost(h_recs);
+    h_recs = nullptr;
+    h_recs_cap = 0;
     if (h_ctl) cudaFreeHost(h_ctl);
     h_ctl = nullptr;
     if (d_slots) cudaFree(d_slots);
@@ -1145,6 +1150,21 @@ struct Engine {
     }
   }
 
+  // The pinned record mirror, grown to n records.
+  vfb_status ensure_recs(int n) {
+    if (n <= h_recs_cap) return VFB_OK;
+    if (cudaStreamSynchronize(stream) != cudaSuccess) return dev_fail(__LINE__);
+    if (h_recs) cudaFreeHost(h_recs);
+    h_recs = nullptr;
+    h_recs_cap = 0;
+    if (cudaMallocHost((void**)&h_recs, (size_t)n * sizeof(InstDev)) != cudaSuccess) {
+      h_recs = nullptr;
+      return VFB_OOM;
+    }
+    h_recs_cap = n;
+    return VFB_OK;
+  }
+
   vfb_status batch(const vfb_instance* ins, int n, vfb_result* out) {
     const auto t0 = std::chrono::steady_clock::now();
     if (n <= 0) return VFB_OK;
@@ -1207,14 +1227,16 @@ struct Engine {
     }
     rc = upload_atoms(ins, H, n, true);
     if (rc == VFB_OK) rc = ensure_workspace(n, chunk_need + n);
+    if (rc == VFB_OK) rc = ensure_recs(n);
     if (rc == VFB_OK) {
-      std::vector<InstDev> recs(n);
-      for (int i = 0; i < n; ++i) recs[i] = H[i].d;
-      if (cudaMemcpyAsync(dInst, recs.data(), (size_t)n * sizeof(InstDev), cudaMemcpyHostToDevice, stream) !=
+      // the records go up from the pinned mirror (the mirror is not written
+      // again before the stream has passed this copy: the results come back
+      // into it after the call's last synchronisation)
+      for (int i = 0; i < n; ++i) h_recs[i] = H[i].d;
+      if (cudaMemcpyAsync(dInst, h_recs, (size_t)n * sizeof(InstDev), cudaMemcpyHostToDevice, stream) !=
           cudaSuccess)
         rc = dev_fail(__LINE__);
       c_h2d += (uint64_t)n * sizeof(InstDev);
-      // pageable source: the copy has been staged when the call returns
     }
     if (rc == VFB_OK) {
       if (profile) cudaEventRecord(ev_k[0], stream);
@@ -1345,9 +1367,14 @@ struct Engine {
       // room for the waits and restarts of a batch under memory pressure)
       if (++guard > 64 * kMaxSize * std::max(1, n)) { rc = dev_fail(__LINE__); break; }
     }
-    // results
-    std::vector<InstDev> recs(n);
-    if (cudaMemcpyAsync(recs.data(), dInst, (size_t)n * sizeof(InstDev), cudaMemcpyDeviceToHost, stream) !=
+    // results (into the pinned mirror when it holds the batch)
+    std::vector<InstDev> recs_pageable;
+    InstDev* recs = h_recs_cap >= n ? h_recs : nullptr;
+    if (!recs) {
+      recs_pageable.resize(n);
+      recs = recs_pageable.data();
+    }
+    if (cudaMemcpyAsync(recs, dInst, (size_t)n * sizeof(InstDev), cudaMemcpyDeviceToHost, stream) !=
             cudaSuccess) {
       if (rc == VFB_OK) rc = dev_fail(__LINE__);
     }
