@@ -439,8 +439,11 @@ struct Engine {
   vfb_status ensure_workspace(int ninst, uint64_t chunk_need) {
     if (ninst > ninst_cap || chunk_need > hB.chunk_cap) {
       if (cudaStreamSynchronize(stream) != cudaSuccess) return dev_fail(__LINE__);
+      // with room to spare: a later call of the same instances starts from
+      // their final capacities (the hints) and needs more chunks at once than
+      // this one did; a reallocation costs a synchronisation and a new graph
       const int nc = std::max(ninst, ninst_cap);
-      const uint64_t cc = std::max<uint64_t>(chunk_need, hB.chunk_cap);
+      const uint64_t cc = std::max<uint64_t>(2 * chunk_need, hB.chunk_cap);
       BatchDev nb{};
       void* p = nullptr;
       const size_t pre = (size_t)(nc + 1) * sizeof(unsigned long long);
