@@ -157,3 +157,22 @@ def test_cli_usage_and_argument_errors(tmp_path):
 def test_cli_strict_exit_codes():
     out = _cli("--strict-exit")
     assert out.returncode == 2
+
+
+def test_problem_c_arrays_follow_assignment():
+    # the C arrays are converted once per Problem; assigning new words or
+    # lengths converts again, and the scalar fields are read at every call
+    prob = vfb_b200.Problem.from_instance(synth.config_planted())
+    s1, keep1 = prob._cstruct()
+    assert list(keep1[0]) == prob.words and list(keep1[1]) == prob.lengths
+    assert [s1.words[i] for i in range(len(prob.words))] == prob.words
+    s1b, keep1b = prob._cstruct()
+    assert keep1b[0] is keep1[0]
+    prob.words = [w ^ 1 for w in prob.words]
+    s2, keep2 = prob._cstruct()
+    assert keep2[0] is not keep1[0]
+    assert [s2.words[i] for i in range(len(prob.words))] == prob.words
+    prob.lengths = list(prob.lengths)
+    prob.max_size = 3
+    s3, keep3 = prob._cstruct()
+    assert keep3[1] is not keep2[1] and s3.max_size == 3 and s3.num_traces == len(prob.lengths)
