@@ -105,3 +105,18 @@ def test_oversubscribed_memory_waits_instead_of_failing():
         results, _, _ = serve.run_stream(eng, [(0.0, p) for p in probs], slots=4, max_steps=20000)
     for got, want in zip(results, full):
         assert _key(got) == _key(want)
+
+
+@pytest.mark.parametrize("arena_mb", [2, 64])
+def test_small_arena_falls_back_to_the_pool(engine, monkeypatch, arena_mb):
+    # a serving session's buffers come from its arena, and from the pool when
+    # no free range of the arena fits: with a tiny arena most growth takes the
+    # pool path, blocks of both kinds are freed and reused within one session,
+    # and every result is still the solo one
+    monkeypatch.setenv("VFB_SERVE_ARENA_MB", str(arena_mb))
+    insts = cases.planted_cases(5) + [synth.config_planted(), cases.random_instance(4242, 4, 5, 5, 16, 8)]
+    insts += cases.small_exact_cases()[:5]
+    stream = [(0.0005 * i, vfb_b200.Problem.from_instance(x)) for i, x in enumerate(insts)]
+    results, _, _ = serve.run_stream(engine, stream, slots=4)
+    for (t, prob), got in zip(stream, results):
+        assert _key(got) == _key(engine.solve(prob))

@@ -1607,8 +1607,18 @@ struct Engine {
     cached_bytes = 0;
     const size_t gran = (size_t)1 << 21;
     size_t want = mem_limit > held_bytes ? (mem_limit - held_bytes) & ~(gran - 1) : 0;
+    size_t least = (size_t)1 << 30;
+    // VFB_SERVE_ARENA_MB caps the arena (a small one makes most blocks come
+    // from the pool: the path a fragmented arena takes)
+    if (const char* cap = std::getenv("VFB_SERVE_ARENA_MB")) {
+      const size_t mb = (size_t)std::strtoull(cap, nullptr, 10);
+      if (mb) {
+        want = std::min(want, (mb << 20) & ~(gran - 1));
+        least = std::min(least, want);
+      }
+    }
     void* p = nullptr;
-    while (want >= ((size_t)1 << 30)) {
+    while (want >= least && want > 0) {
       if (cudaMallocAsync(&p, want, stream) == cudaSuccess) break;
       cudaGetLastError();
       p = nullptr;
