@@ -937,19 +937,20 @@ __device__ void ph_emit_rows(const BatchDev& B, unsigned bid, unsigned nb) {
     const uint64_t r = I.lstart[k] + w;
     uint64_t* dst = I.rows + r * (uint64_t)I.TP;
     const int T = I.T;
-    uint64_t bad = 0;
+    unsigned miss = 0u;   // emit_miss OR-ed over the words (the row's own and ~ X F G step-0 tests)
     for (int t = lane; t < I.TP; t += 32) {
       uint64_t word = 0;
       if (t < T) {
         word = apply_w(c.op, __ldcg(ra + t), __ldcg(rb + t), I.len[t]);
-        bad |= (word ^ (is_pos(I, t) ? 1ULL : 0ULL)) & 1ULL;
+        miss |= emit_miss(word, len_mask(I.len[t]), is_pos(I, t) ? 1u : 0u);
       }
       dst[t] = word;
     }
-    const bool sol = !__any_sync(0xffffffffu, bad != 0);
+    const unsigned m = __reduce_or_sync(0xffffffffu, miss);
     if (lane == 0) {
       I.origin[r] = g;
-      if (sol) atomicMin(&I.best_sol, (unsigned long long)g);
+      if (!(m & 1u)) atomicMin(&I.best_sol, (unsigned long long)g);
+      record_unary(I, k, w, ((m >> 4) & 1u) | (m & 0xEu));   // (~ X F G)
     }
   }
 }
