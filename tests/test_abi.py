@@ -176,3 +176,14 @@ def test_problem_c_arrays_follow_assignment():
     prob.max_size = 3
     s3, keep3 = prob._cstruct()
     assert keep3[1] is not keep2[1] and s3.max_size == 3 and s3.num_traces == len(prob.lengths)
+
+
+def test_problem_pickles_after_a_conversion():
+    import copy
+    import pickle
+    prob = vfb_b200.Problem.from_instance(synth.config_planted())
+    prob._cstruct()
+    again = pickle.loads(pickle.dumps(prob))
+    assert again == prob and copy.deepcopy(prob) == prob
+    s, keep = again._cstruct()
+    assert [s.words[i] for i in range(len(again.words))] == again.words

@@ -198,6 +198,15 @@ class Problem:
             object.__setattr__(self, "_arrays", None)
         object.__setattr__(self, name, value)
 
+    def __getstate__(self):
+        # (the converted copies hold C pointers: not pickled, rebuilt on use)
+        state = dict(self.__dict__)
+        state.pop("_arrays", None)
+        return state
+
+    def __setstate__(self, state):
+        self.__dict__.update(state)
+
     def _cstruct(self):
         # the C arrays are Python array buffers, converted once per Problem
         # (words and lengths are taken as fixed once a Problem has been
