@@ -163,6 +163,8 @@ struct InstDev {
   unsigned long long built_cands, built_wins, built_scanned;
   int built_sol_known;
   int emit_item;                 // owners per k_emit work item at this level (set by the table scan)
+  int no_list;                   // the level has a solution from the start (unary hits): P1 does not
+                                 // list its new slots and the table scan reads the whole table
   // First rows of each stored level whose ~ / X / F / G candidates satisfy
   // the sample (step 0 of every trace equal to its label), stored as
   // 0xFFFFFFFF - row (0: none, so a zeroed record has none); written when

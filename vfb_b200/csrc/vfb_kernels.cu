@@ -287,6 +287,10 @@ __device__ void plan_one(InstDev& I) {
       }
     }
     I.best_cand = first;
+    // a level with a solution from the start and millions of candidates before
+    // it: P1 skips listing its new slots (one atomic per warp and candidate
+    // group) and the table scan reads the whole table instead
+    I.no_list = (first != ~0ULL && first >= (1ULL << 22)) ? 1 : 0;
     I.best_sol = ~0ULL;
     I.n_below = 0;
     I.counted_below = 0;
@@ -442,6 +446,7 @@ __device__ void ph_p1(const BatchDev& B) {
           P.pos[1] = pos1;
           // give up early once the table is known to be too small for this level
           P.otf = __ldcg(&Ip->on_the_fly);
+          P.nolist = __ldcg(&Ip->no_list);
           P.skip = !P.otf && ((fails != 0) || (4 * (keys + fresh) > 3 * cap));
           P.kind = kind;
           // operators whose first candidate in this tile comes after the best
@@ -620,7 +625,7 @@ __device__ void ph_table_scan(const BatchDev& B, unsigned bid, unsigned nb) {
     const unsigned long long k = (unsigned long long)I.level;
     // first attempt at this level with every new slot listed: visit the list;
     // otherwise (a retried level) scan the whole table
-    const bool listed = I.attempt == 1 && I.n_newlist <= I.tent_cap;
+    const bool listed = I.attempt == 1 && !I.no_list && I.n_newlist <= I.tent_cap;
     const uint64_t s0 = (c - B.tscan_prefix[b]) * kScanSlots;
     const uint64_t cap = listed ? I.n_newlist : I.table_mask + 1;
     const uint64_t s1 = (s0 + kScanSlots < cap) ? s0 + kScanSlots : cap;
@@ -993,11 +998,12 @@ __device__ void finish_one(InstDev& I) {
                  cap = I.table_mask + 1, best = I.best_sol, keys = I.keys;
   const uint64_t* wlist = I.wins;
   const uint64_t n_below = I.n_below;
+  const int no_list = I.no_list;
   const int attempt = I.attempt, sol_known = I.sol_known, max_size = I.max_size,
             counted_below = I.counted_below;
   I.built_cands = cands;
   I.built_wins = wins;
-  I.built_scanned = (attempt == 1 && newlist <= tent) ? newlist : cap;
+  I.built_scanned = (attempt == 1 && !no_list && newlist <= tent) ? newlist : cap;
   I.built_sol_known = sol_known;
   I.keys = keys + wins;
   if (best != ~0ULL) {

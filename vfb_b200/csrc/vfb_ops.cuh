@@ -367,6 +367,7 @@ struct TileSh {
   int inst, grp, k, T, TP, half, stride, mode, skip;
   int kind, mask;   // operand group: 0 unary / 1 binary; the operators it evaluates
   int otf;          // on-the-fly level: solution test only, nothing inserted
+  int nolist;       // new slots are not listed (the table scan reads the whole table)
   uint64_t s0, q0, nS, nQ, ni, nj;
   int si, qi;   // levels of the stream / staged operand
   int qleft;    // staged operand is the left operand of & | and of U(i->j)
@@ -404,7 +405,7 @@ struct P1Count {
 template <int N>
 __device__ __forceinline__ void insert_group(InstDev& I, unsigned live, int k, const uint64_t* h,
                                              const uint64_t* l, const uint64_t* g, const uint32_t* bad,
-                                             P1Count& cnt, unsigned valid) {
+                                             P1Count& cnt, unsigned valid, bool list) {
   Slot* tab = I.table;
   const uint64_t mask = I.table_mask;
   uint64_t idx[N];
@@ -425,6 +426,7 @@ __device__ __forceinline__ void insert_group(InstDev& I, unsigned live, int k, c
     if (!bad[j] && g[j] < cnt.sol) cnt.sol = g[j];
   }
   cnt.fresh += nf;
+  if (!list) return;   // (warp-uniform)
   // list the slots of the keys this warp inserted: one atomic per warp, the
   // per-lane offsets from three ballots of the lane's count (0..4)
   const int lane = threadIdx.x & 31;
@@ -589,7 +591,7 @@ __device__ inline void p1_unary(InstDev& I, const TileSh& P, const uint64_t* sS,
   }
 #pragma unroll
   for (int j = 0; j < 4; ++j) bad[j] &= 1u;
-  insert_group<NU>(I, live, P.k, h, l, g, bad, cnt, (unsigned)P.mask);
+  insert_group<NU>(I, live, P.k, h, l, g, bad, cnt, (unsigned)P.mask, !P.nolist);
 }
 
 // KEYS: the operators computed, a prefix of (&, |, laUlb, lbUla) as bits
@@ -648,7 +650,7 @@ __device__ inline void p1_binary(InstDev& I, const TileSh& P, const uint64_t* sS
     if (kV) { key_final<MODE>(kVn, h[3], l[3]); g[3] = I.base_u[P.j] + b * P.ni + a; }
 #pragma unroll
     for (int j = 0; j < 4; ++j) bad[j] &= 1u;
-    insert_group<N>(I, live, P.k, h, l, g, bad, cnt, (unsigned)P.mask & (unsigned)KEYS);
+    insert_group<N>(I, live, P.k, h, l, g, bad, cnt, (unsigned)P.mask & (unsigned)KEYS, !P.nolist);
   }
 }
 
