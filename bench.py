@@ -385,7 +385,7 @@ def serving(local: int, rates: str, count: int):
     import vfb_b200
     from vfb_b200 import serve, synth
     eng = vfb_b200.Engine(device=local, mem_limit_bytes=SERVE_MEM_BYTES)
-    eng.serve_limits(0.8, 0, 1 << 25)
+    eng.serve_limits(0.8, 0, 1 << 23)
     out = []
     for rate in [float(x) for x in rates.split(",") if x]:
         insts = synth.config_serving(4, count, rate, 0.05)

@@ -193,7 +193,7 @@ vfb_status vfb_solve_noalloc(const vfb_instance *inst, vfb_result *out);
  * steps (slices of its operator tiles), so one large request does not hold
  * the others' steps for long.  vfb_serve_limits sets budget_frac (default
  * 0.8), request_bytes (0, the default: a quarter of the budget) and
- * step_candidates (default 2^25; 0: whole levels) for the next
+ * step_candidates (default 2^23; 0: whole levels) for the next
  * vfb_serve_open and the open session.  vfb_serve_open takes the memory
  * budget (less what the engine holds live) from the device in one
  * allocation, halved until it can be had, and the session's buffers are

@@ -395,7 +395,7 @@ class Engine:
 
     # ---- serving (continuous batching)
     def serve_limits(self, budget_frac: float = 0.8, request_bytes: int = 0,
-                     step_candidates: int = 1 << 25) -> None:
+                     step_candidates: int = 1 << 23) -> None:
         """Admission fraction of the memory budget, per-request byte cap (0: budget / 4) and
         operator candidates of one request per step (0: whole levels)."""
         rc = self._lib.vfb_serve_limits(self._ctx, budget_frac, request_bytes, step_candidates)

@@ -71,7 +71,7 @@ constexpr int kBodyLen = 5;   // kernels of one level inside the device-side loo
 constexpr unsigned kMaxLoop = 4 * kMaxSize;
 // serving: P1 candidates of one request per step (a larger level takes
 // several steps), which bounds the step that every resident request waits for
-constexpr uint64_t kServeStepCands = 1ull << 25;
+constexpr uint64_t kServeStepCands = 1ull << 23;
 // candidates of one level above which an instance leaves the cluster solver
 constexpr unsigned long long kPromoteAbove = 1ULL << 21;
 

@@ -111,7 +111,7 @@ def main():
     ap.add_argument("--seed", type=int, default=4)
     ap.add_argument("--large-frac", type=float, default=0.05)
     ap.add_argument("--request-gb", type=float, default=0.0, help="per-request cap (0: budget / 4)")
-    ap.add_argument("--step-cands", type=int, default=1 << 25,
+    ap.add_argument("--step-cands", type=int, default=1 << 23,
                     help="operator candidates of one request per step (0: whole levels)")
     args = ap.parse_args()
     rates = [float(x) for x in args.rates.split(",")] if args.rates else [args.rate]
