@@ -163,6 +163,7 @@ struct InstDev {
   unsigned long long built_cands, built_wins, built_scanned;
   int built_sol_known;
   int emit_item;                 // owners per k_emit work item at this level (set by the table scan)
+  uint32_t scan_slots;           // table-scan chunk of this level's plan (slots; a power of two)
   int no_list;                   // the level has a solution from the start (unary hits): P1 does not
                                  // list its new slots and the table scan reads the whole table
   // First rows of each stored level whose ~ / X / F / G candidates satisfy

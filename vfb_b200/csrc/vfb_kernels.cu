@@ -267,7 +267,12 @@ __device__ void plan_one(InstDev& I) {
   } else {
     I.plan_tiles = t;
     I.plan_words = words;
-    I.plan_tchunks = on_the_fly ? 0 : (table_cap + kScanSlots - 1) / kScanSlots;
+    // scan chunks of kScanSlots, larger on large tables (down to 8192 chunks,
+    // chunks of at most 4 kScanSlots): fewer per-chunk reductions and atomics
+    uint64_t ss = (uint64_t)kScanSlots;
+    while (ss < 4 * (uint64_t)kScanSlots && table_cap / (2 * ss) >= 8192) ss *= 2;
+    I.scan_slots = (uint32_t)ss;
+    I.plan_tchunks = on_the_fly ? 0 : (table_cap + ss - 1) / ss;
     I.planned = k;
     I.p1_done = 0;
     I.p1_step = t;
@@ -606,7 +611,7 @@ __global__ void __launch_bounds__(kTS) k_p1_bulk(BatchDev* Bp) {
 
 // ============================================================== table scan
 // Owners of the keys first seen at level k: every slot whose payload carries
-// level k.  One chunk of kScanSlots slots per CTA iteration; an empty slot's
+// level k.  One chunk of scan_slots slots per CTA iteration; an empty slot's
 // payload (~0) carries no level <= 32.  One warp per instance also settles
 // whether the recorded solution candidate owns its key.
 // The table scan's counting mode at a level that has a solution candidate
@@ -626,9 +631,10 @@ __device__ void ph_table_scan(const BatchDev& B, unsigned bid, unsigned nb) {
     // first attempt at this level with every new slot listed: visit the list;
     // otherwise (a retried level) scan the whole table
     const bool listed = I.attempt == 1 && !I.no_list && I.n_newlist <= I.tent_cap;
-    const uint64_t s0 = (c - B.tscan_prefix[b]) * kScanSlots;
+    const uint64_t ss = I.scan_slots;
+    const uint64_t s0 = (c - B.tscan_prefix[b]) * ss;
     const uint64_t cap = listed ? I.n_newlist : I.table_mask + 1;
-    const uint64_t s1 = (s0 + kScanSlots < cap) ? s0 + kScanSlots : cap;
+    const uint64_t s1 = (s0 + ss < cap) ? s0 + ss : cap;
     // a level with a solution candidate (where it may skip operators) counts
     // the owners below the candidate instead of marking owner bits: if the
     // candidate owns its key (nearly always, and always with exact keys)

@@ -7,7 +7,8 @@ namespace vfb {
 constexpr int kChunkWords = 4096;     // bitmap words per compaction chunk (131072 bits)
 constexpr int kChunkThreads = 256;    // threads per compaction CTA
 constexpr int kScanThreads = 1024;
-constexpr int kScanSlots = 8192;      // hash-set slots per table-scan chunk
+constexpr int kScanSlots = 8192;      // hash-set slots per table-scan chunk (at least; more on
+                                      // tables of over 2^26 slots, see scan_slots)
 constexpr int kScanBatch = 8;         // table-scan entries a thread reads at a time
 constexpr int kCompactWords = 512;    // owner-bitmap words per k_compact chunk (16384 candidates)
 constexpr int kCompactThreads = 256;  // threads per k_compact CTA (two bitmap words each)
