@@ -90,6 +90,7 @@ struct Engine {
   cudaStream_t stream = nullptr;
   int sms = 0;
   int grid = 0;        // grid-stride CTAs (256 threads)
+  int emit_grid = 0;   // k_emit CTAs: two full waves of its resident CTAs
   int p1_grid = 0;     // P1 CTAs
   int adv_threads = 1024;  // k_advance threads (set per captured batch size)
   cudaError_t last_error = cudaSuccess;
@@ -401,6 +402,13 @@ struct Engine {
     for (auto& e : ev_k)
       if (cudaEventCreate(&e) != cudaSuccess) return VFB_DEVICE_ERROR;
     grid = sms * 8;
+    {
+      // k_emit's items are spread over its CTAs evenly, so a grid that is not
+      // a whole number of waves leaves SMs idle in the last one
+      int oe = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&oe, k_emit, 256, 0) != cudaSuccess || oe < 1) oe = 1;
+      emit_grid = sms * oe * 2;
+    }
     const int maxsmem = (kTS * (kMaxTraces + 1) + kTQ * kMaxTraces) * 8;
     if (cudaFuncSetAttribute(k_p1, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsmem) != cudaSuccess)
       return VFB_DEVICE_ERROR;
@@ -527,7 +535,7 @@ struct Engine {
     mark();
     step_launch(pdl, k_compact, (unsigned)(sms * 8), (unsigned)kCompactThreads, 0, dB);
     mark();
-    step_launch(pdl, k_emit, (unsigned)grid, 256u, 0, dB);
+    step_launch(pdl, k_emit, (unsigned)emit_grid, 256u, 0, dB);
     mark();
     step_launch(pdl, k_advance, 1u, (unsigned)adv_threads, 0, dB, handle, built1, lp, mx);
     mark();
